@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the large-ingest workload: R-MAT(0.57,0.19,0.19,0.05) over V=2^17 vertices, 2^30 edge
+updates (~12% deletions of earlier inserts) generated on the device from a seed, with a connected-
+components query after every 2^27 updates (8 ingest phases + 8 queries per step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gs|reference]
+
+One step = clear the V sketches, then 8 x (ingest 2^27 records + connected_components()).  The records
+(8 GiB per GPU) are resident in HBM before timing and larger than L2.  `value` is the edge-update rate
+of the K timed steps (CUDA events on the stream the library launches on; max over ranks); `e2e` is the
+same workload through the C ABI from pinned host buffers (H2D inside the timed region) with the
+component labels copied back after every query.  N > 1 ranks run independent replicas (seed + rank).
+`--impl reference` times the reference's own CPU CCSketchAlg (compiled from its sources into
+oracle/_ref) on a bounded sample of the same stream with every host thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+V_LOG2 = 17
+STREAM_SEED = 0x5EED0002
+SKETCH_SEED = 0xC0FFEE
+METRIC = "edge updates/sec"
+UNIT = "edge_updates/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gs", "reference"], default="gs")
+    ap.add_argument("--updates-log2", type=int, default=30)
+    ap.add_argument("--phase-log2", type=int, default=27)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target wall time of the CPU sample")
+    return ap.parse_args()
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """dram bytes read+write of one full-size ingest launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "k_ingest_rmat17_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_full_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].isdigit():
+                    rows.append(f)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [int(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def cpu_baseline(pairs_host, V, phase, target_s, threads=None):
+    """The reference's CCSketchAlg (oracle/_ref, its own sources) on a bounded prefix of the stream:
+    records bucketed by endpoint into reference-sized batches (outside the timing), then
+    apply_update_batch from T std::threads, plus one connected_components() pro-rated per `phase`."""
+    import numpy as np
+    from oracle import RefCC, bucket_by_vertex
+
+    T = threads or len(os.sched_getaffinity(0))
+    ref = RefCC(V, SKETCH_SEED, 1.0, workers=T)
+    batch = int(ref.L.gsref_cc_desired_batch(ref.h))
+    # calibrate on 2^20 records, then size the sample to ~target_s of ingest
+    cal = np.ascontiguousarray(pairs_host[: 1 << 20])
+    b = bucket_by_vertex(cal, V, batch)
+    t0 = time.perf_counter()
+    ref.ingest_batches(*b, threads=T)
+    rate0 = len(cal) / (time.perf_counter() - t0)
+    n = int(min(len(pairs_host), max(1 << 20, rate0 * target_s)))
+    n = 1 << (n.bit_length() - 1)
+    sample = np.ascontiguousarray(pairs_host[:n])
+    b = bucket_by_vertex(sample, V, batch)
+    t0 = time.perf_counter()
+    ref.ingest_batches(*b, threads=T)
+    t_ing = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    labels, ncc, rounds = ref.connected_components()
+    t_cc = time.perf_counter() - t0
+    ref.close()
+    rate = n / (t_ing + t_cc * n / phase)
+    return {"value": rate, "unit": UNIT, "cores": T, "kind": "reference",
+            "sample": f"first 2^{n.bit_length() - 1} records of the same R-MAT stream, bucketed by endpoint into "
+                      f"{batch}-dst batches (untimed), CCSketchAlg::apply_update_batch from {T} threads "
+                      f"({t_ing:.2f} s) + one connected_components() ({t_cc:.2f} s) pro-rated at one per 2^"
+                      f"{phase.bit_length() - 1} records"}
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    import numpy as np
+    import gpusketch_b200 as gs
+    from oracle import RefCC, bucket_by_vertex, ref_available
+
+    if not ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgsref.so was not built"}))
+        return
+    V = 1 << V_LOG2
+    phase = 1 << args.phase_log2
+    T = len(os.sched_getaffinity(0))
+    # size one step to a bounded sample: calibrate, then ~target s per step
+    n_total = 1 << min(args.updates_log2, 26)
+    pairs = gs.rmat_stream(V_LOG2, n_total, STREAM_SEED)
+    ref = RefCC(V, SKETCH_SEED, 1.0, workers=T)
+    batch = int(ref.L.gsref_cc_desired_batch(ref.h))
+    cal = bucket_by_vertex(pairs[: 1 << 20], V, batch)
+    t0 = time.perf_counter()
+    ref.ingest_batches(*cal, threads=T)
+    rate0 = (1 << 20) / (time.perf_counter() - t0)
+    budget = 150.0 / max(1, args.steps + args.warmup)  # the whole run within a few minutes
+    n = int(min(n_total, max(1 << 20, rate0 * budget)))
+    n = 1 << (n.bit_length() - 1)
+    b = bucket_by_vertex(pairs[:n], V, batch)
+    times = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ref.ingest_batches(*b, threads=T)
+        t1 = time.perf_counter()
+        ref.connected_components()
+        t2 = time.perf_counter()
+        if it >= args.warmup:
+            times.append((t1 - t0) + (t2 - t1) * n / phase)
+    ref.close()
+    sec = sum(times) / len(times)
+    value = n / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "large_ingest_rmat17", "V": V, "updates_per_step": n,
+                   "phase_updates": phase, "sample": True},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": T, "kind": "reference",
+                         "sample": f"2^{n.bit_length() - 1} records per step of the R-MAT stream, bucketed by "
+                                   f"endpoint (untimed); CCSketchAlg::apply_update_batch from {T} threads + "
+                                   f"connected_components() pro-rated at one per 2^{args.phase_log2} records"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gs(args):
+    import numpy as np
+    import torch
+    import gpusketch_b200 as gs
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    V = 1 << V_LOG2
+    U = 1 << args.updates_log2
+    phase = 1 << args.phase_log2
+    P = U // phase
+    stream_seed = STREAM_SEED + rank
+    dev = torch.device("cuda", local)
+
+    d_in = torch.empty((U, 2), dtype=torch.int32, device=dev)
+    gs.rmat_stream(V_LOG2, U, stream_seed, out=d_in)
+    torch.cuda.synchronize()
+
+    g = gs.GraphSketch(V, SKETCH_SEED + rank, device=local, max_batch_edges=phase)
+    ts = torch.cuda.current_stream()
+    g.set_stream(ts)
+    geo = g.geometry
+
+    def step(src):
+        g.clear()
+        for p in range(P):
+            g.ingest_pairs(src[p * phase:(p + 1) * phase])
+            g.connected_components()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step(d_in)
+    torch.cuda.synchronize()
+    g.profile_enable(True)
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(ts)
+        for _ in range(args.steps):
+            step(d_in)
+        end.record(ts)
+        torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(end)
+    prof = g.profile_read()
+    clocks = clk.summary()
+    ms_max = max_over_ranks(ms)
+    ms_per_step = ms_max / args.steps
+    value = world * U * args.steps / (ms_max / 1e3)
+
+    # roofline of the dominant kernel (the sketch update), per launch: B_edge = 8 + 2*V*S_v/U_phase
+    # bytes per edge update (the read half dropped for the first phase of a step, whose sketches are 0)
+    Sv = geo.bytes_per_vertex
+    alg_step = 8.0 * U + V * Sv * (2 * P - 1)
+    alg_per_launch = alg_step / P
+    launches = max(1, prof["ingest_launches"])
+    ingest_ms_avg = prof["ingest_ms"] / launches
+    achieved = alg_per_launch / (ingest_ms_avg / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": ncu_traffic_per_launch(), "peak_source": peak_kind,
+                "kernel": "k_ingest (sketch update)", "alg_bytes_per_launch": alg_per_launch,
+                "avg_launch_ms": ingest_ms_avg, "path_frac": value / world * (alg_step / U) / 1e9 / peak}
+    split = {"ingest_ms_per_step": prof["ingest_ms"] / args.steps, "bucket_ms_per_step": prof["bucket_ms"] / args.steps,
+             "query_ms_per_step": prof["query_ms"] / args.steps}
+
+    e2e = None
+    if not args.no_e2e:
+        h_in = torch.empty((U, 2), dtype=torch.int32, pin_memory=True)
+        h_in.copy_(d_in)
+        labels_host = torch.empty(V, dtype=torch.int32, pin_memory=True)
+
+        def step_e2e():
+            g.clear()
+            for p in range(P):
+                g.ingest_pairs(h_in[p * phase:(p + 1) * phase])   # host pinned -> H2D inside the library
+                labels, _, _ = g.connected_components()           # labels copied back to the host
+        step_e2e()
+        torch.cuda.synchronize()
+        barrier()
+        e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_start.record(ts)
+        for _ in range(args.steps):
+            step_e2e()
+        e_end.record(ts)
+        torch.cuda.synchronize()
+        barrier()
+        ems = max_over_ranks(e_start.elapsed_time(e_end))
+        e2e = {"value": world * U * args.steps / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": U * 8,
+               "d2h_bytes_per_step": P * V * 4, "ms_per_step": ems / args.steps}
+        del h_in
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sample = d_in[: 1 << 26].cpu().numpy().astype(np.uint32)
+            cpu = cpu_baseline(sample, V, phase, args.cpu_seconds)
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference", "sample": f"failed: {exc}"}
+
+    g.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": "large_ingest_rmat17", "V": V, "updates_per_step": U, "phase_updates": phase,
+                   "cc_queries_per_step": P, "rmat": [0.57, 0.19, 0.19, 0.05], "delete_frac": 0.12,
+                   "stream_seed": f"{STREAM_SEED:#x}+rank", "sketch_seed": f"{SKETCH_SEED:#x}+rank",
+                   "sketch_bytes_per_vertex": Sv, "l2": "inputs larger than L2 (8 GiB of records per GPU)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": prof["kernel_launches"],
+        "clocks": clocks, "kernel_split": split,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gs(args)
+
+
+if __name__ == "__main__":
+    main()

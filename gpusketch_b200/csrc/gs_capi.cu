@@ -1,0 +1,589 @@
+// gs_capi.cu - the extern "C" boundary declared in include/gpusketch.h.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "gs_internal.h"
+
+namespace {
+
+// Makes the handle's device current for the duration of a call and restores the caller's.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) { ok = false; return; }
+    if (dev >= 0 && dev != prev) ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define GS_GUARD(g)                                                       \
+  DeviceGuard _guard((g)->device);                                        \
+  if (!_guard.ok) { gs_set_error("cannot select CUDA device"); return GS_ERR_NO_DEVICE; }
+
+cudaStream_t pick_stream(gs_graph* g, void* s) { return s ? static_cast<cudaStream_t>(s) : g->stream; }
+
+void free_graph(gs_graph* g) {
+  if (!g) return;
+  cudaFree(g->d_sk); cudaFree(g->d_colmix);
+  cudaFree(g->d_cnt); cudaFree(g->d_off); cudaFree(g->d_choff); cudaFree(g->d_tile);
+  cudaFree(g->d_nbr); cudaFree(g->d_pairs);
+  if (g->h_pin) cudaFreeHost(g->h_pin);
+  if (g->h_status) cudaFreeHost(g->h_status);
+  cudaFree(g->d_status);
+  cudaFree(g->d_parent); cudaFree(g->d_size); cudaFree(g->d_res); cudaFree(g->d_samp); cudaFree(g->d_acc);
+  cudaFree(g->d_forest);
+  for (int i = 0; i < 2; i++) {
+    if (g->ev_copy[i]) cudaEventDestroy(g->ev_copy[i]);
+    if (g->ev_done[i]) cudaEventDestroy(g->ev_done[i]);
+  }
+  if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
+  if (g->ev_order) cudaEventDestroy(g->ev_order);
+  if (g->own_stream) cudaStreamDestroy(g->own_stream);
+  delete g;
+}
+
+// Checks and clears the device error word after the queued work finished.
+gs_status check_status(gs_graph* g, cudaStream_t s) {
+  GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GS_CUDA_TRY(cudaStreamSynchronize(s));
+  const uint32_t bits = g->h_status[0];
+  if (bits) {
+    GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, sizeof(uint32_t), s));
+    GS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (bits & GS_DEV_ERR_VERTEX_RANGE) {
+      gs_set_error("an edge record named a vertex id >= num_vertices; those records were skipped");
+      return GS_ERR_BAD_ARG;
+    }
+    gs_set_error("device consistency check failed (bits " + std::to_string(bits) + ")");
+    return GS_ERR_INTERNAL;
+  }
+  return GS_OK;
+}
+
+// work queued on a caller stream s must finish before the handle's own stream touches the sketches
+gs_status order_after(gs_graph* g, cudaStream_t s) {
+  if (s == g->stream) return GS_OK;
+  GS_CUDA_TRY(cudaEventRecord(g->ev_order, s));
+  GS_CUDA_TRY(cudaStreamWaitEvent(g->stream, g->ev_order, 0));
+  return GS_OK;
+}
+
+uint64_t staging_pairs(const gs_graph* g) { return std::min<uint64_t>(g->max_batch_edges, 1ull << 25); }
+
+}  // namespace
+
+gs_status gs_ensure_pair_staging(gs_graph* g) {
+  if (g->d_pairs) return GS_OK;
+  const uint64_t cap = staging_pairs(g);
+  GS_CUDA_TRY(cudaMalloc(&g->d_pairs, 2 * cap * 2 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMallocHost(&g->h_pin, 2 * cap * 2 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; i++) {
+    GS_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_copy[i], cudaEventDisableTiming));
+    GS_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_done[i], cudaEventDisableTiming));
+  }
+  g->pairs_cap = cap;
+  return GS_OK;
+}
+
+extern "C" {
+
+gs_status gs_graph_create(const gs_graph_config* cfg, gs_graph** out) {
+  if (!cfg || !out) { gs_set_error("gs_graph_create: null argument"); return GS_ERR_BAD_ARG; }
+  *out = nullptr;
+  if (cfg->num_vertices < 2 || cfg->num_levels < 1 ||
+      (uint64_t)cfg->num_vertices * cfg->num_levels >= (1ull << 32) - 1) {
+    gs_set_error("gs_graph_create: need num_vertices >= 2, num_levels >= 1 and levels*V < 2^32");
+    return GS_ERR_BAD_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    gs_set_error("no CUDA device");
+    return GS_ERR_NO_DEVICE;
+  }
+  int dev = cfg->device;
+  if (dev < 0) cudaGetDevice(&dev);
+  if (dev >= ndev) { gs_set_error("device ordinal out of range"); return GS_ERR_BAD_ARG; }
+  DeviceGuard guard(dev);
+  if (!guard.ok) { gs_set_error("cannot select CUDA device"); return GS_ERR_NO_DEVICE; }
+
+  std::unique_ptr<gs_graph, void (*)(gs_graph*)> g(new gs_graph(), free_graph);
+  g->V = cfg->num_vertices;
+  g->num_levels = cfg->num_levels;
+  g->num_subgraphs = cfg->num_subgraphs ? cfg->num_subgraphs : cfg->num_levels;
+  if (g->num_subgraphs < 1 || g->num_subgraphs > 64) { gs_set_error("num_subgraphs must be in [1, 64]"); return GS_ERR_BAD_ARG; }
+  g->seed = cfg->seed;
+  g->sketches_factor = cfg->sketches_factor > 0 ? cfg->sketches_factor : 1.0;
+  g->batch_factor = cfg->batch_factor > 0 ? cfg->batch_factor : 1.0;
+  g->device = dev;
+  g->max_batch_edges = cfg->max_batch_edges ? cfg->max_batch_edges : (1ull << 27);
+  if (g->max_batch_edges > (1ull << 30)) g->max_batch_edges = 1ull << 30;
+  g->geom = gs_make_geom(g->V, g->sketches_factor);
+  if (g->geom.num_columns > 64) { gs_set_error("more than 64 sketch columns are not supported"); return GS_ERR_BAD_ARG; }
+  cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  g->tune = gs_tune_for(g->geom, g->num_sms);
+  g->sample_cursor.assign(g->num_levels, 0);
+
+  const uint32_t V = g->V, nb = g->geom.num_buckets, bkt = g->geom.bkt_per_col, C = g->geom.num_columns;
+  GS_CUDA_TRY(cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking));
+  g->stream = g->own_stream;
+  GS_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_order, cudaEventDisableTiming));
+  const size_t sk_bytes = (size_t)g->num_levels * V * nb * sizeof(GsBucket);
+  GS_CUDA_TRY(cudaMalloc(&g->d_sk, sk_bytes));
+  GS_CUDA_TRY(cudaMemsetAsync(g->d_sk, 0, sk_bytes, g->stream));
+  std::vector<uint64_t> colmix(C + 1);
+  for (uint32_t c = 0; c < C; c++) colmix[c] = gs_seed_mix(g->seed + 5ull * c);  // column_seed (sketch.h:303)
+  colmix[C] = gs_seed_mix(g->seed);                                                 // checksum_seed (sketch.h:304)
+  GS_CUDA_TRY(cudaMalloc(&g->d_colmix, (C + 1) * sizeof(uint64_t)));
+  GS_CUDA_TRY(cudaMemcpy(g->d_colmix, colmix.data(), (C + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice));
+  GS_CUDA_TRY(cudaMalloc(&g->d_status, 16 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 16 * sizeof(uint32_t), g->stream));
+  GS_CUDA_TRY(cudaMallocHost(&g->h_status, 16 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMalloc(&g->d_parent, (size_t)V * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMalloc(&g->d_size, (size_t)V * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMalloc(&g->d_res, (size_t)V * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMalloc(&g->d_samp, (size_t)V * sizeof(uint64_t)));
+  GS_CUDA_TRY(cudaMalloc(&g->d_acc, (size_t)V * (bkt + 1) * sizeof(GsBucket)));
+  GS_CUDA_TRY(cudaMalloc(&g->d_forest, (size_t)2 * V * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  *out = g.release();
+  return GS_OK;
+}
+
+gs_status gs_graph_destroy(gs_graph* g) {
+  if (!g) return GS_OK;
+  DeviceGuard guard(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  free_graph(g);
+  return GS_OK;
+}
+
+gs_status gs_graph_geometry(const gs_graph* g, gs_geometry* out) {
+  if (!g || !out) { gs_set_error("null argument"); return GS_ERR_BAD_ARG; }
+  out->num_vertices = g->V;
+  out->num_samples = g->geom.num_samples;
+  out->cols_per_sample = 1;
+  out->num_columns = g->geom.num_columns;
+  out->bkt_per_col = g->geom.bkt_per_col;
+  out->num_buckets = g->geom.num_buckets;
+  out->bytes_per_vertex = (uint64_t)g->geom.num_buckets * sizeof(GsBucket);
+  return GS_OK;
+}
+
+gs_status gs_clear(gs_graph* g) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  const size_t bytes = (size_t)g->num_levels * g->V * g->geom.num_buckets * sizeof(GsBucket);
+  GS_CUDA_TRY(cudaMemsetAsync(g->d_sk, 0, bytes, g->stream));
+  g->labels_valid = false;
+  std::fill(g->sample_cursor.begin(), g->sample_cursor.end(), 0u);
+  return GS_OK;
+}
+
+gs_status gs_graph_set_stream(gs_graph* g, void* stream) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  GS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  g->stream = stream ? static_cast<cudaStream_t>(stream) : g->own_stream;
+  return GS_OK;
+}
+
+uint64_t gs_desired_updates_per_batch(const gs_graph* g) {
+  if (!g) return 0;
+  const uint64_t n = (uint64_t)g->geom.num_buckets * sizeof(GsBucket) / sizeof(uint32_t);
+  return (uint64_t)(n * g->batch_factor);
+}
+
+gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int on_device, void* stream) {
+  if (!g || (n && !pairs)) { gs_set_error("gs_ingest_pairs: null argument"); return GS_ERR_BAD_ARG; }
+  if (n == 0) return GS_OK;
+  GS_GUARD(g);
+  cudaStream_t s = pick_stream(g, stream);
+  g->labels_valid = false;
+  if (on_device) {
+    GS_TRY(gs_ingest_device_pairs(g, pairs, n, -1, s));
+    return order_after(g, s);
+  }
+
+  // host input: double-buffered H2D through the pinned ring (or straight from caller memory that
+  // is already page-locked), overlapped with the ingest of the previous slice
+  GS_TRY(gs_ensure_pair_staging(g));
+  cudaPointerAttributes attr{};
+  const bool pinned = cudaPointerGetAttributes(&attr, pairs) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  const uint64_t cap = g->pairs_cap;
+  uint32_t* hp = static_cast<uint32_t*>(g->h_pin);
+  for (uint64_t done = 0, k = 0; done < n; k++) {
+    const uint64_t m = std::min(cap, n - done);
+    const int slot = (int)(k & 1);
+    uint32_t* dslot = g->d_pairs + (size_t)slot * cap * 2;
+    // slice k-2 (same slot) must be consumed before its device and pinned buffers are reused
+    GS_CUDA_TRY(cudaEventSynchronize(g->ev_done[slot]));
+    const uint32_t* src = pairs + 2 * done;
+    if (!pinned) {
+      std::memcpy(hp + (size_t)slot * cap * 2, src, (size_t)m * 2 * sizeof(uint32_t));
+      src = hp + (size_t)slot * cap * 2;
+    }
+    GS_CUDA_TRY(cudaMemcpyAsync(dslot, src, (size_t)m * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                g->copy_stream));
+    GS_CUDA_TRY(cudaEventRecord(g->ev_copy[slot], g->copy_stream));
+    GS_CUDA_TRY(cudaStreamWaitEvent(s, g->ev_copy[slot], 0));
+    GS_TRY(gs_ingest_device_pairs(g, dslot, m, -1, s));
+    GS_CUDA_TRY(cudaEventRecord(g->ev_done[slot], s));
+    done += m;
+  }
+  // the caller's buffer may be reused once every copy has landed
+  GS_CUDA_TRY(cudaStreamSynchronize(g->copy_stream));
+  return order_after(g, s);
+}
+
+gs_status gs_ingest_edges(gs_graph* g, const uint32_t* src, const uint32_t* dst, uint64_t n, int on_device,
+                          void* stream) {
+  if (!g || (n && (!src || !dst))) { gs_set_error("gs_ingest_edges: null argument"); return GS_ERR_BAD_ARG; }
+  if (n == 0) return GS_OK;
+  GS_GUARD(g);
+  std::vector<uint32_t> host;
+  if (on_device) {
+    host.resize(2 * n);
+    std::vector<uint32_t> a(n), b(n);
+    GS_CUDA_TRY(cudaMemcpy(a.data(), src, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    GS_CUDA_TRY(cudaMemcpy(b.data(), dst, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < n; i++) { host[2 * i] = a[i]; host[2 * i + 1] = b[i]; }
+  } else {
+    host.resize(2 * n);
+    for (uint64_t i = 0; i < n; i++) { host[2 * i] = src[i]; host[2 * i + 1] = dst[i]; }
+  }
+  return gs_ingest_pairs(g, host.data(), n, 0, stream);
+}
+
+gs_status gs_ingest_vertex_batches(gs_graph* g, uint32_t level, const uint32_t* srcs, const uint64_t* starts,
+                                   const uint64_t* sizes, uint32_t nbat, const uint32_t* dsts, uint64_t ndst,
+                                   int on_device, void* stream) {
+  if (!g || (nbat && (!srcs || !starts || !sizes)) || (ndst && !dsts)) {
+    gs_set_error("gs_ingest_vertex_batches: null argument");
+    return GS_ERR_BAD_ARG;
+  }
+  if (level >= g->num_levels) { gs_set_error("level out of range"); return GS_ERR_BAD_ARG; }
+  if (nbat == 0) return GS_OK;
+  GS_GUARD(g);
+  cudaStream_t s = pick_stream(g, stream);
+  g->labels_valid = false;
+  if (on_device) {
+    GS_TRY(gs_ingest_device_batches(g, level, srcs, starts, sizes, nbat, dsts, s));
+    return order_after(g, s);
+  }
+  for (uint32_t b = 0; b < nbat; b++) {
+    if (starts[b] > ndst || sizes[b] > ndst - starts[b]) {
+      gs_set_error("gs_ingest_vertex_batches: batch " + std::to_string(b) + " exceeds the dst array");
+      return GS_ERR_BAD_ARG;
+    }
+  }
+  uint32_t *d_srcs = nullptr, *d_dsts = nullptr;
+  uint64_t *d_starts = nullptr, *d_sizes = nullptr;
+  gs_status st = GS_OK;
+  auto fail = [&](cudaError_t e) {
+    gs_set_error(std::string("gs_ingest_vertex_batches: ") + cudaGetErrorString(e));
+    st = e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&d_srcs, nbat * sizeof(uint32_t))) != cudaSuccess) fail(e);
+  else if ((e = cudaMalloc(&d_starts, nbat * sizeof(uint64_t))) != cudaSuccess) fail(e);
+  else if ((e = cudaMalloc(&d_sizes, nbat * sizeof(uint64_t))) != cudaSuccess) fail(e);
+  else if ((e = cudaMalloc(&d_dsts, std::max<uint64_t>(ndst, 1) * sizeof(uint32_t))) != cudaSuccess) fail(e);
+  if (st == GS_OK) {
+    cudaMemcpyAsync(d_srcs, srcs, nbat * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_starts, starts, nbat * sizeof(uint64_t), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_sizes, sizes, nbat * sizeof(uint64_t), cudaMemcpyHostToDevice, s);
+    if (ndst) cudaMemcpyAsync(d_dsts, dsts, ndst * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    st = gs_ingest_device_batches(g, level, d_srcs, d_starts, d_sizes, nbat, d_dsts, s);
+    cudaStreamSynchronize(s);
+  }
+  cudaFree(d_srcs); cudaFree(d_starts); cudaFree(d_sizes); cudaFree(d_dsts);
+  return st;
+}
+
+gs_status gs_synchronize(gs_graph* g) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  if (g->copy_stream) GS_CUDA_TRY(cudaStreamSynchronize(g->copy_stream));
+  return check_status(g, g->stream);
+}
+
+gs_status gs_connected_components(gs_graph* g, uint32_t level, uint32_t* labels, uint32_t* num_cc, uint32_t* rounds) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  if (level >= g->num_levels) { gs_set_error("level out of range"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  cudaStream_t s = g->stream;
+  GS_TRY(check_status(g, s));
+  GS_TRY(gs_boruvka(g, level, 0, s));
+  if (rounds) *rounds = g->last_rounds;
+  if (labels || num_cc) {
+    std::vector<uint32_t> tmp;
+    uint32_t* dst = labels;
+    if (!dst) { tmp.resize(g->V); dst = tmp.data(); }
+    GS_CUDA_TRY(cudaMemcpyAsync(dst, g->d_parent, (size_t)g->V * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (num_cc) {
+      uint32_t c = 0;
+      for (uint32_t v = 0; v < g->V; v++) c += dst[v] == v;
+      *num_cc = c;
+    }
+  }
+  return GS_OK;
+}
+
+gs_status gs_point_query(gs_graph* g, uint32_t a, uint32_t b, int* connected) {
+  if (!g || !connected || a >= g->V || b >= g->V) { gs_set_error("gs_point_query: bad arguments"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  if (!g->labels_valid || g->labels_level != 0) GS_TRY(gs_connected_components(g, 0, nullptr, nullptr, nullptr));
+  uint32_t ra = 0, rb = 0;
+  GS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  GS_CUDA_TRY(cudaMemcpy(&ra, g->d_parent + a, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  GS_CUDA_TRY(cudaMemcpy(&rb, g->d_parent + b, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  *connected = ra == rb;
+  return GS_OK;
+}
+
+gs_status gs_spanning_forest(gs_graph* g, uint32_t level, uint32_t* edges, uint64_t* num_edges) {
+  if (!g || !edges || !num_edges) { gs_set_error("gs_spanning_forest: null argument"); return GS_ERR_BAD_ARG; }
+  GS_TRY(gs_connected_components(g, level, nullptr, nullptr, nullptr));
+  GS_GUARD(g);
+  *num_edges = g->last_forest_edges;
+  GS_CUDA_TRY(cudaMemcpy(edges, g->d_forest, (size_t)2 * g->last_forest_edges * sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost));
+  return GS_OK;
+}
+
+gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, uint32_t* edges, uint64_t* sizes) {
+  if (!g || !edges || !sizes || k == 0) { gs_set_error("gs_disjoint_spanning_forests: bad arguments"); return GS_ERR_BAD_ARG; }
+  if (level >= g->num_levels) { gs_set_error("level out of range"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  cudaStream_t s = g->stream;
+  GS_TRY(check_status(g, s));
+  const uint32_t V = g->V;
+  const size_t stride = 2 * (size_t)(V - 1);
+  uint32_t* d_all = nullptr;
+  GS_CUDA_TRY(cudaMalloc(&d_all, std::max<size_t>(1, k * stride) * sizeof(uint32_t)));
+  uint64_t total = 0;
+  gs_status st = GS_OK;
+  uint32_t done = 0;
+  for (uint32_t j = 0; j < k; j++) {
+    // a min-cut graph samples round 0 at the column its stored sample index reached; a
+    // connected-components graph resets it before every query (CCSketchAlg::connected_components)
+    const uint32_t col0 = g->num_levels > 1 ? g->sample_cursor[level]++ : 0;
+    st = gs_boruvka(g, level, col0, s);
+    if (st != GS_OK) break;
+    const uint32_t ne = g->last_forest_edges;
+    sizes[j] = ne;
+    cudaMemcpyAsync(d_all + total * 2, g->d_forest, (size_t)2 * ne * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(edges + j * stride, g->d_forest, (size_t)2 * ne * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    // filter_sf_edges: XOR the forest out of both endpoint sketches of this level
+    st = gs_ingest_device_pairs(g, d_all + total * 2, ne, (int)level, s);
+    total += ne;
+    done++;
+    if (st != GS_OK) break;
+  }
+  // re-insert every forest found so far (src/mc_sketch_alg.cpp:904-907)
+  gs_status st2 = total ? gs_ingest_device_pairs(g, d_all, total, (int)level, s) : GS_OK;
+  cudaStreamSynchronize(s);
+  cudaFree(d_all);
+  for (uint32_t j = done; j < k; j++) sizes[j] = 0;
+  g->labels_valid = false;
+  if (st != GS_OK) return st;
+  if (st2 != GS_OK) return st2;
+  GS_CUDA_TRY(cudaGetLastError());
+  return check_status(g, s);
+}
+
+gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_found, uint64_t* cut_at_level,
+                     uint8_t* side) {
+  if (!g || !value || k == 0) { gs_set_error("gs_min_cut: bad arguments"); return GS_ERR_BAD_ARG; }
+  const uint32_t V = g->V;
+  std::vector<uint32_t> edges((size_t)k * 2 * (V - 1));
+  std::vector<uint64_t> sizes(k);
+  for (uint32_t lvl = 0; lvl < g->num_levels; lvl++) {
+    GS_TRY(gs_disjoint_spanning_forests(g, lvl, k, edges.data(), sizes.data()));
+    std::vector<uint32_t> cert;
+    for (uint32_t f = 0; f < k; f++)
+      cert.insert(cert.end(), edges.begin() + (size_t)f * 2 * (V - 1),
+                  edges.begin() + (size_t)f * 2 * (V - 1) + 2 * sizes[f]);
+    const uint64_t cut = gs_exact_min_cut_host(V, cert.data(), cert.size() / 2, side);
+    if (cut < k || lvl + 1 == g->num_levels) {
+      *value = cut << lvl;
+      if (level_found) *level_found = lvl;
+      if (cut_at_level) *cut_at_level = cut;
+      return GS_OK;
+    }
+  }
+  return GS_ERR_INTERNAL;
+}
+
+gs_status gs_download_sketches(gs_graph* g, uint32_t level, uint32_t first, uint32_t count, void* host_out) {
+  if (!g || !host_out || level >= g->num_levels || (uint64_t)first + count > g->V) {
+    gs_set_error("gs_download_sketches: bad arguments");
+    return GS_ERR_BAD_ARG;
+  }
+  GS_GUARD(g);
+  GS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  const size_t nb = g->geom.num_buckets;
+  GS_CUDA_TRY(cudaMemcpy(host_out, g->d_sk + ((size_t)level * g->V + first) * nb, (size_t)count * nb * sizeof(GsBucket),
+                         cudaMemcpyDeviceToHost));
+  return GS_OK;
+}
+
+gs_status gs_upload_sketches(gs_graph* g, uint32_t level, uint32_t first, uint32_t count, const void* host_in) {
+  if (!g || !host_in || level >= g->num_levels || (uint64_t)first + count > g->V) {
+    gs_set_error("gs_upload_sketches: bad arguments");
+    return GS_ERR_BAD_ARG;
+  }
+  GS_GUARD(g);
+  GS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  const size_t nb = g->geom.num_buckets;
+  GS_CUDA_TRY(cudaMemcpy(g->d_sk + ((size_t)level * g->V + first) * nb, host_in, (size_t)count * nb * sizeof(GsBucket),
+                         cudaMemcpyHostToDevice));
+  g->labels_valid = false;
+  return GS_OK;
+}
+
+gs_status gs_write_binary(gs_graph* g, const char* path) {
+  if (!g || !path) { gs_set_error("gs_write_binary: null argument"); return GS_ERR_BAD_ARG; }
+  FILE* f = std::fopen(path, "wb");
+  if (!f) { gs_set_error(std::string("cannot open ") + path); return GS_ERR_IO; }
+  const uint64_t seed = g->seed;
+  const uint32_t V = g->V;
+  const double factor = g->sketches_factor;
+  bool ok = std::fwrite(&seed, 8, 1, f) == 1 && std::fwrite(&V, 4, 1, f) == 1 && std::fwrite(&factor, 8, 1, f) == 1;
+  const size_t nb = g->geom.num_buckets;
+  const uint32_t step = (uint32_t)std::max<size_t>(1, (64u << 20) / (nb * sizeof(GsBucket)));
+  std::vector<GsBucket> buf((size_t)step * nb);
+  for (uint32_t v = 0; ok && v < V; v += step) {
+    const uint32_t c = std::min(step, V - v);
+    gs_status st = gs_download_sketches(g, 0, v, c, buf.data());
+    if (st != GS_OK) { std::fclose(f); return st; }
+    ok = std::fwrite(buf.data(), sizeof(GsBucket), (size_t)c * nb, f) == (size_t)c * nb;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) { gs_set_error(std::string("write failed: ") + path); return GS_ERR_IO; }
+  return GS_OK;
+}
+
+gs_status gs_read_binary(const char* path, int32_t device, gs_graph** out) {
+  if (!path || !out) { gs_set_error("gs_read_binary: null argument"); return GS_ERR_BAD_ARG; }
+  FILE* f = std::fopen(path, "rb");
+  if (!f) { gs_set_error(std::string("cannot open ") + path); return GS_ERR_IO; }
+  uint64_t seed = 0;
+  uint32_t V = 0;
+  double factor = 1;
+  if (std::fread(&seed, 8, 1, f) != 1 || std::fread(&V, 4, 1, f) != 1 || std::fread(&factor, 8, 1, f) != 1) {
+    std::fclose(f);
+    gs_set_error("truncated header");
+    return GS_ERR_IO;
+  }
+  gs_graph_config cfg{};
+  cfg.num_vertices = V;
+  cfg.num_levels = 1;
+  cfg.seed = seed;
+  cfg.sketches_factor = factor;
+  cfg.batch_factor = 1;
+  cfg.device = device;
+  gs_graph* g = nullptr;
+  gs_status st = gs_graph_create(&cfg, &g);
+  if (st != GS_OK) { std::fclose(f); return st; }
+  const size_t nb = g->geom.num_buckets;
+  const uint32_t step = (uint32_t)std::max<size_t>(1, (64u << 20) / (nb * sizeof(GsBucket)));
+  std::vector<GsBucket> buf((size_t)step * nb);
+  for (uint32_t v = 0; v < V; v += step) {
+    const uint32_t c = std::min(step, V - v);
+    if (std::fread(buf.data(), sizeof(GsBucket), (size_t)c * nb, f) != (size_t)c * nb) {
+      std::fclose(f);
+      gs_graph_destroy(g);
+      gs_set_error("truncated sketch data");
+      return GS_ERR_IO;
+    }
+    st = gs_upload_sketches(g, 0, v, c, buf.data());
+    if (st != GS_OK) { std::fclose(f); gs_graph_destroy(g); return st; }
+  }
+  std::fclose(f);
+  *out = g;
+  return GS_OK;
+}
+
+gs_status gs_gen_rmat_stream(uint32_t log2_v, double a, double b, double c, double delete_frac, uint64_t seed,
+                             uint64_t first, uint64_t n, uint32_t* pairs, int on_device, void* stream) {
+  if ((n && !pairs) || log2_v < 1 || log2_v > 31 || a < 0 || b < 0 || c < 0 || a + b + c > 1) {
+    gs_set_error("gs_gen_rmat_stream: bad arguments");
+    return GS_ERR_BAD_ARG;
+  }
+  if (on_device) {
+    GS_TRY(gs_gen_rmat_device(log2_v, a, b, c, delete_frac, seed, first, n, pairs, static_cast<cudaStream_t>(stream)));
+    return GS_OK;
+  }
+  gs_gen_rmat_host(log2_v, a, b, c, delete_frac, seed, first, n, pairs);
+  return GS_OK;
+}
+
+}  // extern "C"
+
+// ---- profiling ----
+
+GsProfScope::GsProfScope(gs_graph* g_, int cls_, cudaStream_t s_, uint32_t launches) : g(g_), cls(cls_), s(s_) {
+  g->prof_launches[cls] += launches;
+  g->launches_total += launches;
+  if (!g->prof_on) return;
+  auto& ev = g->prof_ev[cls];
+  const size_t i = g->prof_used[cls];
+  if (ev.size() < 2 * (i + 1)) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return;
+    ev.push_back(a);
+    ev.push_back(b);
+  }
+  if (cudaEventRecord(ev[2 * i], s) != cudaSuccess) return;
+  idx = (long)i;
+  g->prof_used[cls] = i + 1;
+}
+
+GsProfScope::~GsProfScope() {
+  if (idx >= 0) cudaEventRecord(g->prof_ev[cls][2 * idx + 1], s);
+}
+
+extern "C" gs_status gs_profile_enable(gs_graph* g, int enable) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  DeviceGuard guard(g->device);
+  cudaStreamSynchronize(g->stream);
+  g->prof_on = enable != 0;
+  for (int c = 0; c < 3; c++) { g->prof_used[c] = 0; g->prof_launches[c] = 0; }
+  g->launches_total = 0;
+  g->records_total = 0;
+  return GS_OK;
+}
+
+extern "C" gs_status gs_profile_read(gs_graph* g, gs_profile* out) {
+  if (!g || !out) { gs_set_error("null argument"); return GS_ERR_BAD_ARG; }
+  DeviceGuard guard(g->device);
+  GS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+  double ms[3] = {0, 0, 0};
+  for (int c = 0; c < 3; c++) {
+    for (size_t i = 0; i < g->prof_used[c]; i++) {
+      float t = 0;
+      GS_CUDA_TRY(cudaEventElapsedTime(&t, g->prof_ev[c][2 * i], g->prof_ev[c][2 * i + 1]));
+      ms[c] += t;
+    }
+  }
+  out->ingest_launches = g->prof_launches[GS_PROF_INGEST];
+  out->ingest_ms = ms[GS_PROF_INGEST];
+  out->bucket_launches = g->prof_launches[GS_PROF_BUCKET];
+  out->bucket_ms = ms[GS_PROF_BUCKET];
+  out->query_launches = g->prof_launches[GS_PROF_QUERY];
+  out->query_ms = ms[GS_PROF_QUERY];
+  out->kernel_launches = g->launches_total;
+  out->records_ingested = g->records_total;
+  return GS_OK;
+}

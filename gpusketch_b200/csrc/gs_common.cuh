@@ -1,0 +1,134 @@
+// gs_common.cuh - types, hashing and error plumbing shared by the sm_100a kernels and the host.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "../../include/gpusketch.h"
+
+#if defined(__CUDACC__)
+#define GS_HD __host__ __device__ __forceinline__
+#else
+#define GS_HD inline
+#endif
+
+// Bucket {alpha, gamma} (include/bucket.h:7-12).  16-byte aligned so a bucket moves as one
+// 128-bit load/store; the reference packs the same two u64s, so the byte layout is identical.
+struct alignas(16) GsBucket {
+  uint64_t alpha;
+  uint64_t gamma;
+};
+static_assert(sizeof(GsBucket) == 16, "bucket must be 16 bytes");
+
+// ----------------------------------------------------------------------------------------
+// XXH3_64bits_withSeed on an 8-byte little-endian key (include/types.h:8-9), restated from the
+// published xxHash algorithm (XXH3_len_4to8_64b followed by the rrmxmx avalanche).
+//
+// With k' = (key >> 32) | (key << 32) and B(seed) = kSecret64[8..16) ^ kSecret64[16..24) - seed',
+// the first mixing step x = y ^ rotl(y,49) ^ rotl(y,24) of y = k' ^ B is linear over XOR, so
+//     x = mix(k') ^ mix(B(seed)),   mix(z) = z ^ rotl(z,49) ^ rotl(z,24).
+// mix(k') depends only on the edge, mix(B) only on the seed: the ingest kernel computes mix(k')
+// once per record and each column's hash is one XOR plus the two multiplies of gs_hash_tail.
+// ----------------------------------------------------------------------------------------
+constexpr uint64_t kGsSecret8to24 = 0x1cad21f72c81017cULL ^ 0xdb979083e96dd4deULL;
+constexpr uint64_t kGsMx2 = 0x9FB21C651E98DF25ULL;
+
+GS_HD uint64_t gs_rotl64(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+
+GS_HD uint64_t gs_mix(uint64_t z) { return z ^ gs_rotl64(z, 49) ^ gs_rotl64(z, 24); }
+
+// mix(k') for key k
+GS_HD uint64_t gs_key_mix(uint64_t key) { return gs_mix((key >> 32) | (key << 32)); }
+
+// mix(B(seed)) for seed s
+GS_HD uint64_t gs_seed_mix(uint64_t seed) {
+  uint32_t lo = (uint32_t)seed;
+  uint32_t sw = ((lo & 0xffu) << 24) | ((lo & 0xff00u) << 8) | ((lo >> 8) & 0xff00u) | (lo >> 24);
+  uint64_t s = seed ^ ((uint64_t)sw << 32);
+  return gs_mix(kGsSecret8to24 - s);
+}
+
+// rrmxmx after the rotate-xor step: h = x*M; h ^= (h>>35)+8; h *= M; return h ^ (h>>28).
+// (h>>35) < 2^29, so +8 never carries out of the low word and the xor only touches it.
+GS_HD uint64_t gs_hash_tail(uint64_t x) {
+  uint64_t h = x * kGsMx2;
+  uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
+  lo ^= (hi >> 3) + 8u;
+  h = ((uint64_t)hi << 32) | lo;
+  h *= kGsMx2;
+  return h ^ (h >> 28);
+}
+
+GS_HD uint64_t gs_xxh3_8(uint64_t key, uint64_t seed) {
+  return gs_hash_tail(gs_key_mix(key) ^ gs_seed_mix(seed));
+}
+
+// concat_pairing_fn (src/util.cpp:45-51)
+GS_HD uint64_t gs_concat(uint32_t a, uint32_t b) {
+  uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+  return ((uint64_t)lo << 32) | hi;
+}
+
+#if defined(__CUDACC__)
+// ctz(hash | 1<<max_depth) = min(ctz(hash), max_depth), from the tail of the hash
+// (Bucket_Boruvka::get_index_depth, include/bucket.h:54-59).  Computes only the low word of the
+// final xorshift unless it is zero (probability 2^-32).
+__device__ __forceinline__ uint32_t gs_depth_from_mixed(uint64_t x, uint32_t max_depth) {
+  uint64_t h = x * kGsMx2;
+  uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
+  lo ^= (hi >> 3) + 8u;
+  h = ((uint64_t)hi << 32) | lo;
+  h *= kGsMx2;
+  uint32_t l2 = (uint32_t)h, h2 = (uint32_t)(h >> 32);
+  uint32_t flo = l2 ^ __funnelshift_r(l2, h2, 28);
+  uint32_t d;
+  if (flo != 0u) {
+    d = (uint32_t)(__ffs(flo) - 1);
+  } else {
+    uint32_t fhi = h2 ^ (h2 >> 28);
+    d = fhi ? 32u + (uint32_t)(__ffs(fhi) - 1) : 64u;
+  }
+  return d < max_depth ? d : max_depth;
+}
+#endif
+
+// ----------------------------------------------------------------------------------------
+// Sketch geometry (include/sketch.h:177-191,312-320; src/sketch.cpp:24-30)
+// ----------------------------------------------------------------------------------------
+struct GsGeom {
+  uint32_t V;
+  uint32_t num_samples;
+  uint32_t num_columns;
+  uint32_t bkt_per_col;
+  uint32_t num_buckets;
+};
+
+GsGeom gs_make_geom(uint32_t V, double sketches_factor);
+
+// Thread-local error message behind gs_last_error().
+void gs_set_error(const std::string& msg);
+
+#define GS_CUDA_TRY(expr)                                                                    \
+  do {                                                                                       \
+    cudaError_t _e = (expr);                                                                 \
+    if (_e != cudaSuccess) {                                                                 \
+      gs_set_error(std::string(#expr) + ": " + cudaGetErrorString(_e) + " @" + __FILE__ +     \
+                   ":" + std::to_string(__LINE__));                                          \
+      return _e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA;                     \
+    }                                                                                        \
+  } while (0)
+
+#define GS_TRY(expr)                     \
+  do {                                   \
+    gs_status _s = (expr);               \
+    if (_s != GS_OK) return _s;          \
+  } while (0)
+
+// Device-side error word bits (read back by the host after a phase).
+enum : uint32_t {
+  GS_DEV_ERR_VERTEX_RANGE = 1u,   // an input vertex id >= V
+  GS_DEV_ERR_CAPACITY = 2u,       // more records than the scratch holds
+  GS_DEV_ERR_DSU_LIMIT = 4u,      // a DSU walk exceeded its iteration bound
+};

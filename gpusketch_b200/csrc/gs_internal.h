@@ -1,0 +1,114 @@
+// gs_internal.h - the gs_graph handle and the launchers shared by the library's .cu files.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "gs_common.cuh"
+
+// Ingest tuning knobs (picked per geometry by gs_tune_for; overridable through
+// gs_set_tuning for the autotuner).
+struct GsTuning {
+  uint32_t chunk;            // records per work item; larger vertices are split across warps
+  uint32_t warps_per_block;  // warps in an ingest block
+  uint32_t blocks_per_sm;    // resident ingest blocks per SM the grid is sized for
+};
+
+struct gs_graph {
+  // ---- configuration ----
+  GsGeom geom{};
+  uint32_t V = 0;
+  uint32_t num_levels = 1;
+  uint32_t num_subgraphs = 1;  // min-cut tag bound L
+  uint64_t seed = 0;
+  double sketches_factor = 1.0;
+  double batch_factor = 1.0;
+  int device = 0;
+  int num_sms = 148;
+  uint64_t max_batch_edges = 1ull << 27;
+  GsTuning tune{};
+  cudaStream_t stream = nullptr;      // stream every kernel of this handle is launched on
+  cudaStream_t own_stream = nullptr;  // created with the handle
+  cudaEvent_t ev_order = nullptr;     // orders the handle's stream after a caller-stream ingest
+
+  // ---- resident state ----
+  GsBucket* d_sk = nullptr;    // [num_levels][V][num_buckets]
+  uint64_t* d_colmix = nullptr;  // [num_columns] mix(B(seed+5c)), then [num_columns] = mix(B(seed))
+
+  // ---- ingest scratch ----
+  uint64_t nv_cap = 0;         // virtual vertices the per-vertex arrays hold (num_levels*V)
+  uint32_t* d_cnt = nullptr;   // [nv+1] records per virtual vertex, then cursors
+  uint32_t* d_off = nullptr;   // [nv+1] exclusive scan of d_cnt
+  uint32_t* d_choff = nullptr; // [nv+1] exclusive scan of d_nch
+  uint32_t* d_tile = nullptr;  // [2*tiles] per-tile sums for the scan
+  uint32_t* d_nbr = nullptr;   // [nbr_cap] neighbour of each record, grouped by virtual vertex
+  uint64_t nbr_cap = 0;
+  uint32_t* d_pairs = nullptr; // staging for host-resident input pairs, 2 x [pairs_cap] u32 pairs
+  uint64_t pairs_cap = 0;
+  void* h_pin = nullptr;       // 2 pinned staging buffers of pairs_cap pairs
+  cudaStream_t copy_stream = nullptr;               // H2D of host input slices
+  cudaEvent_t ev_copy[2] = {nullptr, nullptr};      // slice copied into d_pairs[slot]
+  cudaEvent_t ev_done[2] = {nullptr, nullptr};      // slice in d_pairs[slot] consumed
+  uint32_t* d_status = nullptr;  // [0] error bits [1] records [2] chunks [3] modified [4] count
+  uint32_t* h_status = nullptr;  // pinned mirror
+
+  // ---- Boruvka scratch ----
+  uint32_t* d_parent = nullptr;  // [V]
+  uint32_t* d_size = nullptr;    // [V]
+  uint32_t* d_res = nullptr;     // [V] sample result code
+  uint64_t* d_samp = nullptr;    // [V] sampled edge id
+  GsBucket* d_acc = nullptr;     // [V][bkt_per_col+1] merged column + deterministic bucket
+  uint32_t* d_forest = nullptr;  // [2*(V-1)] forest edges of the last Boruvka run
+  uint32_t last_forest_edges = 0;
+  uint32_t last_rounds = 0;
+  std::vector<uint32_t> sample_cursor;  // per level: round-0 column of the next k-forest
+  bool labels_valid = false;     // d_parent holds the partition of the last query
+  uint32_t labels_level = 0;
+
+  // ---- profiling ----
+  bool prof_on = false;
+  std::vector<cudaEvent_t> prof_ev[3];   // [class] begin/end pairs: 0 ingest, 1 bucketing, 2 query
+  size_t prof_used[3] = {0, 0, 0};
+  uint64_t prof_launches[3] = {0, 0, 0};
+  uint64_t launches_total = 0;
+  uint64_t records_total = 0;
+};
+
+enum GsProfClass { GS_PROF_INGEST = 0, GS_PROF_BUCKET = 1, GS_PROF_QUERY = 2 };
+
+// Brackets a group of `launches` kernel launches of one class with CUDA events on stream s.
+struct GsProfScope {
+  gs_graph* g;
+  int cls;
+  long idx = -1;
+  cudaStream_t s;
+  GsProfScope(gs_graph* g_, int cls_, cudaStream_t s_, uint32_t launches);
+  ~GsProfScope();
+};
+
+// Partial-support helpers implemented in the .cu files.
+gs_status gs_ensure_ingest_scratch(gs_graph* g, uint64_t records);
+gs_status gs_ensure_pair_staging(gs_graph* g);
+
+// Ingest n edge records already on the device (interleaved pairs).  fixed_level < 0: every level
+// the edge tags into (min-cut) or level 0 (connected components); >= 0: that level only.
+gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t n, int fixed_level,
+                                 cudaStream_t s);
+// Directed per-vertex batches (already on the device).
+gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* d_srcs,
+                                   const uint64_t* d_starts, const uint64_t* d_sizes,
+                                   uint32_t nb, const uint32_t* d_dsts, cudaStream_t s);
+// Device Boruvka on one level; forest edges stay in g->d_forest.
+gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s);
+
+// Exact global min cut (host), gs_mincut.cpp.
+uint64_t gs_exact_min_cut_host(uint32_t V, const uint32_t* pairs, uint64_t m, uint8_t* side);
+
+// R-MAT record generator shared by host and device (gs_gen.cu).
+gs_status gs_gen_rmat_device(uint32_t log2_v, double a, double b, double c, double delete_frac,
+                             uint64_t seed, uint64_t first, uint64_t n, uint32_t* d_pairs,
+                             cudaStream_t s);
+void gs_gen_rmat_host(uint32_t log2_v, double a, double b, double c, double delete_frac,
+                      uint64_t seed, uint64_t first, uint64_t n, uint32_t* pairs);
+
+GsTuning gs_tune_for(const GsGeom& geom, int num_sms);

@@ -1,0 +1,230 @@
+/*
+ * gpusketch.h - C ABI of the B200 graph-stream sketching engine.
+ *
+ * Every entry point takes plain pointers and sizes, returns a gs_status and never
+ * throws or exits.  The library owns all device memory; host pointers are borrowed
+ * for the duration of a call.  A gs_graph handle is not thread-safe: use one thread
+ * per handle or serialise calls.  Distinct handles may be used concurrently.
+ *
+ * Terms (the reference's domain vocabulary):
+ *   vertex sketch   num_buckets Buckets {u64 alpha; u64 gamma} (16 B, packed) laid out as
+ *                   num_columns columns of bkt_per_col buckets followed by one
+ *                   deterministic bucket (reference include/bucket.h:7-12,
+ *                   src/sketch.cpp:8-22,85-99).
+ *   sketch set      [num_levels][num_vertices][num_buckets] Buckets in HBM.  A connected-
+ *                   components graph has one level; a min-cut graph keeps one level per
+ *                   sketched subgraph (reference src/mc_sketch_alg.cpp:93-122).
+ *   edge record     one stream update (insert or delete) of the undirected edge {src,dst};
+ *                   it XOR-toggles the edge id (min<<32)|max in both endpoint sketches
+ *                   (reference src/cc_sketch_alg.cpp:154-160, src/util.cpp:45-51).
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   include/cuda_kernel.cuh:23-51     SketchParams, CudaKernel::sketchUpdate
+ *   include/cuda_stream.h:146-276     CudaStream::process_batch / flush_buffers
+ *   src/cc_gpu_sketch_alg.cpp:7-31    CCGPUSketchAlg::apply_update_batch / flush_buffers
+ *   src/cc_sketch_alg.cpp:491-683     boruvka_emulation, connected_components, point_query,
+ *                                     calc_spanning_forest, write_binary
+ *   src/mc_sketch_alg.cpp:738-1002    k_boruvka_emulation, calc_disjoint_spanning_forests,
+ *                                     calc_minimum_cut
+ *   src/mc_gpu_sketch_alg.cpp:139-178 MCGPUSketchAlg::apply_update_batch (subgraph tagging)
+ */
+#ifndef GPUSKETCH_H_
+#define GPUSKETCH_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_ABI_VERSION 1
+
+typedef enum gs_status {
+  GS_OK = 0,
+  GS_ERR_BAD_ARG = 1,        /* invalid argument or out-of-range vertex id */
+  GS_ERR_CUDA = 2,           /* CUDA runtime error (message in gs_last_error) */
+  GS_ERR_OOM = 3,            /* device or pinned host allocation failed */
+  GS_ERR_SKETCH_FAIL = 4,    /* Boruvka ran out of sketch columns (OutOfSamplesException) */
+  GS_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up */
+  GS_ERR_UPDATE_LOCKED = 6,  /* update while a query holds the sketches (UpdateLockedException) */
+  GS_ERR_IO = 7,             /* file read/write failed */
+  GS_ERR_INTERNAL = 8,       /* device-side consistency check failed */
+  GS_ERR_NO_DEVICE = 9       /* no CUDA device or the kernels were not built for it */
+} gs_status;
+
+/* Bucket as stored in device memory and in the checkpoint file (include/bucket.h:7-12). */
+typedef struct gs_bucket {
+  uint64_t alpha; /* XOR of edge ids */
+  uint64_t gamma; /* XOR of XXH3(edge id, seed) checksums */
+} gs_bucket;
+
+/* Sketch geometry derived exactly as the reference does (include/sketch.h:177-191,312-320,
+ * src/sketch.cpp:24-30): num_samples = max(18, ceil(f*log2(V)/0.736965594)),
+ * cols_per_sample = 1, bkt_per_col = ceil(log2(V(V-1)/2))+1 (bumped by one when a
+ * multiple of 16), num_buckets = num_columns*bkt_per_col + 1. */
+typedef struct gs_geometry {
+  uint32_t num_vertices;
+  uint32_t num_samples;
+  uint32_t cols_per_sample;
+  uint32_t num_columns;
+  uint32_t bkt_per_col;
+  uint32_t num_buckets;
+  uint64_t bytes_per_vertex; /* num_buckets * 16 */
+} gs_geometry;
+
+/* Host-only sizing; replaces Sketch::calc_vector_length / calc_cc_samples /
+ * calc_bkt_per_col (include/sketch.h:177-191,312-320). */
+gs_status gs_geometry_for(uint32_t num_vertices, double sketches_factor, gs_geometry* out);
+
+/* Host reference of the 8-byte XXH3_64bits_withSeed used for every column, checksum and
+ * subgraph hash (include/types.h:8-9, include/bucket.h:54-63). */
+uint64_t gs_hash64(uint64_t key, uint64_t seed);
+
+typedef struct gs_graph_config {
+  uint32_t num_vertices;   /* V; vertex ids are [0, V) */
+  uint32_t num_levels;     /* 1 = connected-components graph; >1 = min-cut subgraph levels */
+  uint64_t seed;           /* sketch seed; column c hashes with seed+5c, checksum with seed */
+  double sketches_factor;  /* CCAlgConfiguration::sketches_factor (<=0 means 1) */
+  double batch_factor;     /* CCAlgConfiguration::batch_factor (<=0 means 1) */
+  uint32_t num_subgraphs;  /* min-cut tag bound L: level = ctz(XXH3(e,seed) | 1<<(L-1)); 0 = num_levels */
+  int32_t device;          /* CUDA device ordinal; -1 = current device */
+  uint64_t max_batch_edges;/* edges per internal ingest pass; 0 = library default (2^27) */
+} gs_graph_config;
+
+typedef struct gs_graph gs_graph;
+
+/* Allocates zeroed sketches for every level (CCSketchAlg / MCSketchAlg constructors,
+ * src/cc_sketch_alg.cpp:11-55, src/mc_sketch_alg.cpp:16-40,93-122). */
+gs_status gs_graph_create(const gs_graph_config* cfg, gs_graph** out);
+gs_status gs_graph_destroy(gs_graph* g);
+gs_status gs_graph_geometry(const gs_graph* g, gs_geometry* out);
+/* Zeroes every sketch of the set (Sketch::zero_contents over all vertices, src/sketch.cpp:102-108). */
+gs_status gs_clear(gs_graph* g);
+/* Makes the handle launch on `cuda_stream` (cudaStream_t; NULL restores its own stream), so the
+ * caller's CUDA events on that stream bracket the handle's kernels. */
+gs_status gs_graph_set_stream(gs_graph* g, void* cuda_stream);
+/* Updates per worker batch the reference would buffer: bucket_array_bytes/4*batch_factor
+ * (include/cc_sketch_alg.h:147-151). */
+uint64_t gs_desired_updates_per_batch(const gs_graph* g);
+
+/* Ingest n edge records given as interleaved uint32 pairs [src0,dst0,src1,dst1,...].
+ * Each record toggles edge {src,dst} in both endpoint sketches of every level the edge
+ * tags into (one level for connected-components graphs).  Self-loops are no-ops, as in
+ * the reference where the two updates of sketch src cancel.  pairs_on_device != 0 means
+ * `pairs` is a device pointer; otherwise it is host memory (pinned or pageable) staged
+ * through the library's pinned ring.  `cuda_stream` (cudaStream_t, may be NULL) orders the
+ * work after the caller's stream.  Replaces the GPU worker path
+ * GraphSketchDriver::batch_callback -> CCGPUSketchAlg::apply_update_batch ->
+ * CudaStream::process_batch -> CudaKernel::sketchUpdate (include/graph_sketch_driver.h:204-208,
+ * src/cc_gpu_sketch_alg.cpp:7-19, include/cuda_stream.h:146-202, src/cuda_kernel.cu:242-257). */
+gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int pairs_on_device,
+                          void* cuda_stream);
+
+/* Same as gs_ingest_pairs with separate src / dst arrays. */
+gs_status gs_ingest_edges(gs_graph* g, const uint32_t* src, const uint32_t* dst, uint64_t n,
+                          int on_device, void* cuda_stream);
+
+/* The reference's per-vertex batch form: batch b XORs edges (srcs[b], dsts[starts[b] + i]),
+ * i < sizes[b], into the sketch of srcs[b] ONLY, at sketch level `level`
+ * (CCSketchAlg::apply_update_batch, src/cc_sketch_alg.cpp:133-145;
+ * CudaKernel::sketchUpdate inputs, include/cuda_kernel.cuh:46). */
+gs_status gs_ingest_vertex_batches(gs_graph* g, uint32_t level, const uint32_t* srcs,
+                                   const uint64_t* starts, const uint64_t* sizes,
+                                   uint32_t num_batches, const uint32_t* dsts,
+                                   uint64_t num_dsts, int on_device, void* cuda_stream);
+
+/* Waits until every queued update is applied (CCGPUSketchAlg::flush_buffers,
+ * src/cc_gpu_sketch_alg.cpp:21-31; MCGPUSketchAlg::apply_flush_updates). */
+gs_status gs_synchronize(gs_graph* g);
+
+/* Device Boruvka emulation on sketch level `level` (CCSketchAlg::connected_components,
+ * src/cc_sketch_alg.cpp:491-584).  labels (host, length V, may be NULL) receives the minimum
+ * vertex id of each vertex's component; num_cc and rounds may be NULL.  Returns
+ * GS_ERR_SKETCH_FAIL when the sketch runs out of columns. */
+gs_status gs_connected_components(gs_graph* g, uint32_t level, uint32_t* labels, uint32_t* num_cc,
+                                  uint32_t* rounds);
+
+/* CCSketchAlg::point_query (src/cc_sketch_alg.cpp:630-672). */
+gs_status gs_point_query(gs_graph* g, uint32_t a, uint32_t b, int* connected);
+
+/* Spanning forest found by the last Boruvka run on `level` (calc_spanning_forest,
+ * src/cc_sketch_alg.cpp:586-595).  edges (host) holds 2*(V-1) uint32 as (src<dst) pairs. */
+gs_status gs_spanning_forest(gs_graph* g, uint32_t level, uint32_t* edges, uint64_t* num_edges);
+
+/* k edge-disjoint spanning forests of sketch level `level`: after each forest its edges are
+ * XOR-deleted from the level's sketches, and all are re-inserted at the end
+ * (MCSketchAlg::calc_disjoint_spanning_forests / filter_sf_edges,
+ * src/mc_sketch_alg.cpp:837-919).  edges (host) holds k*2*(V-1) uint32, forest f starting at
+ * offset f*2*(V-1); forest_sizes[f] receives its edge count. */
+gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, uint32_t* edges,
+                                       uint64_t* forest_sizes);
+
+/* Min-cut driver of the reference's tools/min_cut.cu:208-252: for level g = 0,1,... take k
+ * disjoint spanning forests, compute the exact minimum cut of their union, and stop at the
+ * first level whose cut is < k (or at the last level).  value = cut * 2^g.  side (host,
+ * length V, may be NULL) receives 1 for vertices on one side of the cut. */
+gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_found,
+                     uint64_t* cut_at_level, uint8_t* side);
+
+/* Exact global minimum cut of an undirected multigraph given as uint32 pairs (host).
+ * Replaces the VieCut call of MCSketchAlg::calc_minimum_cut (src/mc_sketch_alg.cpp:966-1002). */
+gs_status gs_exact_min_cut(uint32_t num_vertices, const uint32_t* pairs, uint64_t num_edges,
+                           uint64_t* value, uint8_t* side);
+
+/* Copy vertex sketches [first, first+count) of `level` to / from host memory in the
+ * contiguous [vertex][num_buckets] Bucket layout of Sketch::serialize
+ * (src/sketch.cpp:204-206). */
+gs_status gs_download_sketches(gs_graph* g, uint32_t level, uint32_t first_vertex, uint32_t count,
+                               void* host_out);
+gs_status gs_upload_sketches(gs_graph* g, uint32_t level, uint32_t first_vertex, uint32_t count,
+                             const void* host_in);
+
+/* Checkpoint in the reference's format: [u64 seed][u32 V][f64 sketches_factor] then
+ * V*num_buckets Buckets of level 0 (CCSketchAlg::write_binary, src/cc_sketch_alg.cpp:674-683;
+ * construct_from_serialized_data, :57-91). */
+gs_status gs_write_binary(gs_graph* g, const char* path);
+gs_status gs_read_binary(const char* path, int32_t device, gs_graph** out);
+
+/* ---- profiling (per-handle CUDA-event timing on the stream each kernel is launched on) ---- */
+typedef struct gs_profile {
+  uint64_t ingest_launches;  /* sketch-update kernel launches */
+  double ingest_ms;          /* their summed event-timed duration */
+  uint64_t bucket_launches;  /* endpoint-bucketing kernel launches (count, scan, scatter) */
+  double bucket_ms;
+  uint64_t query_launches;   /* Boruvka kernel launches */
+  double query_ms;
+  uint64_t kernel_launches;  /* every kernel this handle launched */
+  uint64_t records_ingested; /* edge records consumed by the ingest path */
+} gs_profile;
+
+/* Resets the counters; when `enable` is non-zero, brackets each kernel group with CUDA events.
+ * Library extension without a reference counterpart (the reference times with std::chrono,
+ * include/cuda_stream.h:286-291). */
+gs_status gs_profile_enable(gs_graph* g, int enable);
+/* Waits for queued work and returns the counters accumulated since gs_profile_enable. */
+gs_status gs_profile_read(gs_graph* g, gs_profile* out);
+
+/* Last error message of the calling thread ("" when none). */
+const char* gs_last_error(void);
+
+/* ---- seeded synthetic streams (test and benchmark inputs; not reference code) ---- */
+
+/* Erdos-Renyi G(V, p) edges in shuffled order, then a `delete_frac` share deleted and a
+ * `reinsert_frac` share of those re-inserted.  Host-side; writes at most `capacity` pairs
+ * and returns the record count in *n. */
+gs_status gs_gen_er_stream(uint32_t num_vertices, double p, uint64_t seed, double delete_frac,
+                           double reinsert_frac, uint32_t* pairs, uint64_t capacity, uint64_t* n);
+
+/* R-MAT(a,b,c) stream over 2^log2_v vertices, records [first, first+n) of the counter-based
+ * stream with a `delete_frac` share of records deleting an earlier inserted edge.  Runs on
+ * the device when pairs_on_device != 0 (pairs is a device pointer), else on the host. */
+gs_status gs_gen_rmat_stream(uint32_t log2_v, double a, double b, double c, double delete_frac,
+                             uint64_t seed, uint64_t first, uint64_t n, uint32_t* pairs,
+                             int pairs_on_device, void* cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUSKETCH_H_ */

@@ -1,0 +1,296 @@
+"""GPU parity: device sketches bit-identical to the oracle / the reference's own CCSketchAlg, and
+connected components, forests and min cuts equal to exact answers.  All calls go through the C ABI."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import gpusketch_b200 as gs
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_SEED = 0xC0FFEE
+
+
+def sketch_bytes(g: gs.GraphSketch, level: int = 0) -> bytes:
+    return g.download(level).tobytes()
+
+
+def oracle_bytes(R, V, seed, pairs, factor=1.0) -> bytes:
+    sk = R.new_sketches(V, factor)
+    R.ingest(sk, V, seed, pairs, factor)
+    return sk.tobytes()
+
+
+def case_pairs(name, golden_dir):
+    if name == "plain_cc_er1024":
+        return gs.er_stream(1024, 0.05, 0x5EED0001, 0.10, 0.5)
+    if name == "multiples_1024":
+        return np.load(os.path.join(golden_dir, "multiples_1024_stream.npy"))
+    if name == "er256_sparse":
+        return gs.er_stream(256, 0.01, 11, 0.5, 0.2)
+    if name == "er4096":
+        return gs.er_stream(4096, 0.002, 13, 0.1, 0.5)
+    return gs.rmat_stream(12, 40000, 0x5EED0002)
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available(), "gpu tests need a CUDA device"
+    return torch
+
+
+def test_plain_cc_config(restatement, golden_dir):
+    """ER G(1024, 0.05), 10% deleted, half re-inserted; sketch seed 0xC0FFEE; default params."""
+    case = json.load(open(os.path.join(golden_dir, "ref_digests.json")))[0]
+    pairs = case_pairs("plain_cc_er1024", golden_dir)
+    with gs.GraphSketch(1024, PLAIN_SEED) as g:
+        g.ingest_pairs(pairs)
+        g.synchronize()
+        b = sketch_bytes(g)
+        assert hashlib.sha256(b).hexdigest() == case["sketch_sha256"]   # the reference's write_binary bytes
+        assert b == oracle_bytes(restatement, 1024, PLAIN_SEED, pairs)
+        labels, ncc, rounds = g.connected_components()
+    exact_n, exact_labels = restatement.exact_cc(1024, pairs)
+    assert ncc == exact_n == case["num_cc"]
+    assert np.array_equal(labels, exact_labels)
+    assert rounds == case["rounds"]
+
+
+@pytest.mark.parametrize("device_input", [False, True])
+def test_reference_digests(restatement, golden_dir, device_input, torch_cuda):
+    for case in json.load(open(os.path.join(golden_dir, "ref_digests.json"))):
+        pairs = case_pairs(case["name"], golden_dir)
+        V, seed = case["V"], int(case["seed"])
+        with gs.GraphSketch(V, seed) as g:
+            if device_input:
+                g.ingest_pairs(torch_cuda.from_numpy(pairs.astype(np.int32)).cuda())
+            else:
+                g.ingest_pairs(pairs)
+            g.synchronize()
+            assert hashlib.sha256(sketch_bytes(g)).hexdigest() == case["sketch_sha256"], case["name"]
+            labels, ncc, rounds = g.connected_components()
+        assert ncc == case["num_cc"] and rounds == case["rounds"], case["name"]
+        _, exact = restatement.exact_cc(V, pairs)
+        assert np.array_equal(labels, exact), case["name"]
+
+
+@pytest.mark.parametrize("V,seed", [(2, 1), (3, 2**64 - 1), (17, 0), (256, 2**63), (1000, 12345),
+                                    (4096, 0xDEADBEEFCAFEBABE), (16384, 77)])
+def test_random_streams_bit_exact(restatement, V, seed):
+    rng = np.random.default_rng(V * 7 + 1)
+    n = min(60000, 30 * V)
+    pairs = rng.integers(0, V, size=(n, 2), dtype=np.uint32)
+    if V > 8:
+        pairs = pairs[(pairs[:, 0] % 3) == (pairs[:, 1] % 3)]  # several components
+    with gs.GraphSketch(V, seed) as g:
+        g.ingest_pairs(pairs)
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs)
+        labels, ncc, rounds = g.connected_components()
+    sk = restatement.new_sketches(V)
+    restatement.ingest(sk, V, seed, pairs)
+    st, olabels, orounds, _ = restatement.boruvka(sk, V, seed)
+    assert st == 0 and np.array_equal(labels, olabels) and rounds == orounds
+    assert ncc == restatement.exact_cc(V, pairs)[0]
+
+
+def test_hub_vertex_spans_many_chunks(restatement):
+    """A vertex with > 3 work chunks of records merges through the atomic path."""
+    V, seed = 20000, 99
+    star = np.stack([np.zeros(V - 1, np.uint32), np.arange(1, V, dtype=np.uint32)], 1)
+    rng = np.random.default_rng(4)
+    noise = rng.integers(0, V, size=(40000, 2), dtype=np.uint32)
+    pairs = np.concatenate([star, noise, star[:5000]])          # 5000 star edges toggled off again
+    with gs.GraphSketch(V, seed) as g:
+        g.ingest_pairs(pairs)
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs)
+        labels, ncc, _ = g.connected_components()
+    n, exact = restatement.exact_cc(V, pairs)
+    assert ncc == n and np.array_equal(labels, exact)
+
+
+def test_more_than_32_columns(restatement):
+    """sketches_factor 3 at V=4096 gives 49 columns: two columns per lane."""
+    V, seed, f = 4096, 5, 3.0
+    assert gs.geometry_for(V, f).num_columns > 32
+    rng = np.random.default_rng(9)
+    pairs = rng.integers(0, V, size=(50000, 2), dtype=np.uint32)
+    with gs.GraphSketch(V, seed, sketches_factor=f) as g:
+        g.ingest_pairs(pairs)
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs, f)
+        labels, _, _ = g.connected_components()
+    assert np.array_equal(labels, restatement.exact_cc(V, pairs)[1])
+
+
+def test_vertex_batches_apply_to_source_only(restatement):
+    """apply_update_batch(src, dsts) XORs (src,dst) into src's sketch only, self-loops included."""
+    V, seed = 512, 31
+    rng = np.random.default_rng(6)
+    srcs = rng.integers(0, V, 300).astype(np.uint32)
+    sizes = rng.integers(0, 700, 300).astype(np.uint64)
+    starts = np.zeros_like(sizes)
+    np.cumsum(sizes[:-1], out=starts[1:])
+    dsts = rng.integers(0, V, int(sizes.sum())).astype(np.uint32)
+    dsts[:5] = srcs[0]
+    with gs.GraphSketch(V, seed) as g:
+        g.ingest_vertex_batches(srcs, starts, sizes, dsts)
+        got = sketch_bytes(g)
+    geo = restatement.geometry(V)
+    nb = geo["num_buckets"]
+    sk = restatement.new_sketches(V)
+    for b in range(len(srcs)):
+        s = int(srcs[b])
+        one = sk[s * nb * 2:(s + 1) * nb * 2]
+        for d in dsts[int(starts[b]):int(starts[b] + sizes[b])].tolist():
+            e = (min(s, d) << 32) | max(s, d)
+            restatement.sketch_update(one, V, seed, e)
+    assert got == sk.tobytes()
+
+
+def test_linearity_and_self_inverse(restatement):
+    V, seed = 3000, 2024
+    rng = np.random.default_rng(7)
+    A = rng.integers(0, V, size=(30000, 2), dtype=np.uint32)
+    B = rng.integers(0, V, size=(20000, 2), dtype=np.uint32)
+    with gs.GraphSketch(V, seed) as g1, gs.GraphSketch(V, seed) as g2:
+        g1.ingest_pairs(A); g1.ingest_pairs(B)
+        g2.ingest_pairs(B); g2.ingest_pairs(np.concatenate([A[::-1]]))
+        assert sketch_bytes(g1) == sketch_bytes(g2)
+        g1.ingest_pairs(A); g1.ingest_pairs(B)
+        assert not np.frombuffer(sketch_bytes(g1), np.uint64).any()   # merging the same delta twice gives ZERO
+
+
+def test_edge_cases(restatement):
+    V, seed = 100, 3
+    with gs.GraphSketch(V, seed) as g:
+        g.ingest_pairs(np.empty((0, 2), np.uint32))
+        g.ingest_pairs(np.array([[5, 5], [7, 7]], np.uint32))      # self-loops cancel
+        assert not np.frombuffer(sketch_bytes(g), np.uint64).any()
+        labels, ncc, rounds = g.connected_components()
+        assert ncc == V and rounds == 0                           # every sample is ZERO
+        bad = np.array([[1, 2], [3, 100], [4, 5]], np.uint32)      # vertex 100 is out of range
+        g.ingest_pairs(bad)
+        with pytest.raises(gs.GpuSketchError) as e:
+            g.synchronize()
+        assert e.value.status == 1
+        good = np.array([[1, 2], [4, 5]], np.uint32)
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, good)
+        assert g.point_query(1, 2) and g.point_query(4, 5) and not g.point_query(1, 4)
+
+
+def test_spanning_forest_and_disjoint_forests(restatement):
+    V, seed = 2000, 8
+    pairs = gs.er_stream(V, 0.004, 21, 0.2, 0.5)
+    final = {tuple(e) for e in restatement.final_edges(V, pairs).tolist()}
+    with gs.GraphSketch(V, seed) as g:
+        g.ingest_pairs(pairs)
+        before = sketch_bytes(g)
+        f = g.spanning_forest()
+        ncc_exact, exact = restatement.exact_cc(V, pairs)
+        assert len(f) == V - ncc_exact and {tuple(e) for e in f.tolist()} <= final
+        n2, lab2 = restatement.cc_of_edges(V, f)
+        assert np.array_equal(lab2, exact)
+        forests = g.disjoint_spanning_forests(3)
+        assert sketch_bytes(g) == before                              # deletions were reverted
+    remaining = set(final)
+    for fo in forests:
+        fe = {tuple(e) for e in fo.tolist()}
+        assert fe <= remaining
+        rem = np.asarray(sorted(remaining), np.uint32).reshape(-1, 2)
+        n1, l1 = restatement.cc_of_edges(V, rem)
+        n2, l2 = restatement.cc_of_edges(V, fo)
+        assert np.array_equal(l1, l2) and len(fo) == V - n1
+        remaining -= fe
+
+
+def test_min_cut_levels_bit_exact(restatement):
+    """Subgraph tagging: each edge goes to levels 0..min(tag, levels-1)."""
+    V, seed, levels, L = 600, 17, 5, 19
+    rng = np.random.default_rng(12)
+    pairs = rng.integers(0, V, size=(20000, 2), dtype=np.uint32)
+    with gs.GraphSketch(V, seed, num_levels=levels, num_subgraphs=L) as g:
+        g.ingest_pairs(pairs)
+        got = b"".join(sketch_bytes(g, lv) for lv in range(levels))
+    sk = restatement.new_sketches(V, levels=levels)
+    restatement.ingest_levels(sk, V, levels, L, seed, pairs)
+    assert got == sk.tobytes()
+
+
+def test_min_cut_planted_cut():
+    """Two dense ER blocks joined by a planted cut of 3 edges: min cut 3 at level 0."""
+    n, seed = 150, 0x5EED0003
+    rng = np.random.default_rng(13)
+    blocks = []
+    for off in (0, n):
+        a, b = np.triu_indices(n, 1)
+        keep = rng.random(a.size) < 0.3
+        blocks.append(np.stack([a[keep] + off, b[keep] + off], 1))
+    cut = np.stack([rng.integers(0, n, 3), rng.integers(n, 2 * n, 3)], 1)
+    pairs = np.concatenate(blocks + [cut]).astype(np.uint32)
+    pairs = pairs[rng.permutation(len(pairs))]
+    V = 2 * n
+    L = 1 + 2 * int(np.log2(V))
+    alg = gs.MCGPUSketchAlg(V, seed, num_subgraphs=L, max_sketch_graphs=4, k=4)
+    alg.ingest_pairs(pairs)
+    value, level, cut_at = alg.min_cut()
+    assert (value, level, cut_at) == (3, 0, 3)
+
+
+def test_checkpoint_roundtrip(restatement, tmp_path, golden_dir):
+    case = json.load(open(os.path.join(golden_dir, "ref_digests.json")))[1]
+    pairs = case_pairs("multiples_1024", golden_dir)
+    path = str(tmp_path / "ck.bin")
+    with gs.GraphSketch(1024, PLAIN_SEED) as g:
+        g.ingest_pairs(pairs)
+        g.write_binary(path)
+    data = open(path, "rb").read()
+    assert data[:20] == PLAIN_SEED.to_bytes(8, "little") + (1024).to_bytes(4, "little") + np.float64(1.0).tobytes()
+    assert hashlib.sha256(data[20:]).hexdigest() == case["sketch_sha256"]
+    g2 = gs.GraphSketch.read_binary(path)
+    labels, ncc, _ = g2.connected_components()
+    g2.close()
+    assert ncc == 78
+
+
+def test_reference_named_api(restatement, golden_dir):
+    pairs = case_pairs("multiples_1024", golden_dir)
+    alg = gs.CCGPUSketchAlg(1024, PLAIN_SEED, gs.CCAlgConfiguration().batch_factor(1), num_threads=4)
+    # worker batches the way the driver delivers them: both directions, per source vertex
+    src = np.concatenate([pairs[:, 0], pairs[:, 1]])
+    dst = np.concatenate([pairs[:, 1], pairs[:, 0]])
+    for v in np.unique(src):
+        alg.apply_update_batch(int(v) % 4, int(v), dst[src == v])
+    cc = alg.connected_components()
+    assert cc.size() == 78
+    ids = {frozenset(s) for s in cc.get_component_sets()}
+    assert frozenset({2, 4, 6}) <= next(s for s in ids if 2 in s)
+    assert alg.point_query(3, 9) and not alg.point_query(3, 5)
+
+
+def test_full_size_rmat_properties(restatement, torch_cuda):
+    """V=2^17 R-MAT, 2^24 records generated on the device: exact partition, and per-vertex sketches
+    of sampled vertices equal to their oracle sketch built from the vertex's own records."""
+    torch = torch_cuda
+    V, seed, n = 1 << 17, 0x5EED0002, 1 << 24
+    d = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+    gs.rmat_stream(17, n, 0x5EED0002, out=d)
+    host = d.cpu().numpy().astype(np.uint32)
+    with gs.GraphSketch(V, seed) as g:
+        g.ingest_pairs(d[: n // 2])
+        g.ingest_pairs(d[n // 2:])
+        labels, ncc, rounds = g.connected_components()
+        sample = [0, 1, 2, 3, 1000, 65535, 131071]
+        got = g.download()
+    nexact, exact = restatement.exact_cc(V, host)
+    assert ncc == nexact and np.array_equal(labels, exact)
+    nb = restatement.geometry(V)["num_buckets"]
+    for v in sample:
+        mine = host[(host[:, 0] == v) | (host[:, 1] == v)]
+        mine = mine[mine[:, 0] != mine[:, 1]]
+        one = np.zeros(nb * 2, np.uint64)
+        for a, b in mine.tolist():
+            restatement.sketch_update(one, V, seed, (min(a, b) << 32) | max(a, b))
+        assert got[v].tobytes() == one.tobytes(), v
