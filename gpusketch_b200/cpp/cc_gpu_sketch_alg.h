@@ -1,0 +1,174 @@
+// cc_gpu_sketch_alg.h - CCGPUSketchAlg drop-in: the reference's connected-components algorithm
+// interface (include/cc_sketch_alg.h:65-261, include/cc_gpu_sketch_alg.h:8-110) over the C ABI.
+//
+// The sketches live on the GPU for the lifetime of the object.  Worker-thread batches handed to
+// apply_update_batch (thread-safe, as the driver contract requires, include/graph_sketch_driver.h:49-52)
+// are buffered per call site and shipped in bulk through gs_ingest_vertex_batches, the way the
+// reference's CudaStream gathers ~540 batches per kernel launch (include/cc_gpu_sketch_alg.h:20).
+// Bulk edge records (the device-bucketed path) go through ingest_records.
+#pragma once
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gpusketch_types.h"
+
+class CCGPUSketchAlg {
+ public:
+  CCGPUSketchAlg(node_id_t num_vertices, size_t seed, CCAlgConfiguration config = CCAlgConfiguration(),
+                 int device = -1)
+      : num_vertices(num_vertices), seed(seed), config(config) {
+    gs_graph_config cfg{};
+    cfg.num_vertices = num_vertices;
+    cfg.num_levels = 1;
+    cfg.seed = seed;
+    cfg.sketches_factor = config.get_sketches_factor();
+    cfg.batch_factor = config.get_batch_factor();
+    cfg.device = device;
+    gs_throw_if(gs_graph_create(&cfg, &g), "gs_graph_create");
+    flush_at = 540 * get_desired_updates_per_batch();
+  }
+
+  ~CCGPUSketchAlg() { gs_graph_destroy(g); }
+  CCGPUSketchAlg(const CCGPUSketchAlg&) = delete;
+  CCGPUSketchAlg& operator=(const CCGPUSketchAlg&) = delete;
+
+  // construct_from_serialized_data (src/cc_sketch_alg.cpp:57-70)
+  static CCGPUSketchAlg* construct_from_serialized_data(const std::string& input_file,
+                                                        CCAlgConfiguration config = CCAlgConfiguration()) {
+    gs_graph* h = nullptr;
+    gs_throw_if(gs_read_binary(input_file.c_str(), -1, &h), "gs_read_binary");
+    gs_geometry geo{};
+    gs_graph_geometry(h, &geo);
+    return new CCGPUSketchAlg(h, geo.num_vertices, config);
+  }
+
+  // ---- driver contract (include/graph_sketch_driver.h:28-69) ----
+  void allocate_worker_memory(size_t num_workers) { (void)num_workers; }
+  size_t get_desired_updates_per_batch() { return gs_desired_updates_per_batch(g); }
+  node_id_t get_num_vertices() { return num_vertices; }
+  void pre_insert(GraphUpdate, int = 0) {}           // no eager DSU: queries always run Boruvka
+  bool has_cached_query(int) { return false; }
+  void print_configuration() { std::cout << config << std::endl; }
+
+  void apply_update_batch(int thr_id, node_id_t src_vertex, const std::vector<node_id_t>& dst_vertices) {
+    (void)thr_id;
+    std::lock_guard<std::mutex> lk(mtx);
+    if (update_locked) throw UpdateLockedException();
+    srcs.push_back(src_vertex);
+    starts.push_back(dsts.size());
+    sizes.push_back(dst_vertices.size());
+    dsts.insert(dsts.end(), dst_vertices.begin(), dst_vertices.end());
+    if (dsts.size() >= flush_at) ship_locked();
+  }
+
+  // CCGPUSketchAlg::flush_buffers (src/cc_gpu_sketch_alg.cpp:21-31)
+  void flush_buffers() {
+    std::lock_guard<std::mutex> lk(mtx);
+    ship_locked();
+    gs_throw_if(gs_synchronize(g), "gs_synchronize");
+  }
+
+  // CCSketchAlg::update (src/cc_sketch_alg.cpp:154-160): both endpoint sketches
+  void update(GraphUpdate upd) {
+    uint32_t p[2] = {upd.edge.src, upd.edge.dst};
+    ingest_records(p, 1);
+  }
+
+  // n edge records as interleaved (src, dst) pairs in host memory
+  void ingest_records(const uint32_t* pairs, size_t n) {
+    std::lock_guard<std::mutex> lk(mtx);
+    gs_throw_if(gs_ingest_pairs(g, pairs, n, 0, nullptr), "gs_ingest_pairs");
+  }
+
+  // ---- queries (src/cc_sketch_alg.cpp:542-683) ----
+  ConnectedComponents connected_components() {
+    flush_buffers();
+    std::vector<node_id_t> labels(num_vertices);
+    uint32_t ncc = 0, rounds = 0;
+    gs_throw_if(gs_connected_components(g, 0, labels.data(), &ncc, &rounds), "gs_connected_components");
+    last_query_rounds = rounds;
+    return ConnectedComponents(std::move(labels));
+  }
+
+  bool point_query(node_id_t a, node_id_t b) {
+    flush_buffers();
+    int c = 0;
+    gs_throw_if(gs_point_query(g, a, b, &c), "gs_point_query");
+    return c != 0;
+  }
+
+  SpanningForest calc_spanning_forest() {
+    flush_buffers();
+    std::vector<uint32_t> e(2 * (size_t)num_vertices);
+    uint64_t n = 0;
+    gs_throw_if(gs_spanning_forest(g, 0, e.data(), &n), "gs_spanning_forest");
+    return SpanningForest(to_edges(e.data(), n));
+  }
+
+  std::vector<SpanningForest> calc_disjoint_spanning_forests(size_t k) {
+    flush_buffers();
+    const size_t stride = 2 * (size_t)(num_vertices - 1);
+    std::vector<uint32_t> e(k * stride);
+    std::vector<uint64_t> sizes(k);
+    gs_throw_if(gs_disjoint_spanning_forests(g, 0, (uint32_t)k, e.data(), sizes.data()),
+                "gs_disjoint_spanning_forests");
+    std::vector<SpanningForest> out;
+    for (size_t f = 0; f < k; f++) out.emplace_back(to_edges(e.data() + f * stride, sizes[f]));
+    return out;
+  }
+
+  void write_binary(const std::string& filename) {
+    flush_buffers();
+    gs_throw_if(gs_write_binary(g, filename.c_str()), "gs_write_binary");
+  }
+
+  // getters (include/cc_sketch_alg.h:256-260)
+  size_t get_seed() { return seed; }
+  size_t max_rounds() {
+    gs_geometry geo{};
+    gs_graph_geometry(g, &geo);
+    return geo.num_samples;
+  }
+  bool get_update_locked() { return update_locked; }
+  gs_graph* handle() { return g; }
+
+  size_t last_query_rounds = 0;
+
+ private:
+  CCGPUSketchAlg(gs_graph* h, node_id_t V, CCAlgConfiguration cfg) : num_vertices(V), seed(0), config(cfg), g(h) {
+    flush_at = 540 * get_desired_updates_per_batch();
+  }
+
+  static std::vector<Edge> to_edges(const uint32_t* e, uint64_t n) {
+    std::vector<Edge> out(n);
+    for (uint64_t i = 0; i < n; i++) out[i] = {e[2 * i], e[2 * i + 1]};
+    return out;
+  }
+
+  void ship_locked() {
+    if (srcs.empty()) return;
+    gs_throw_if(gs_ingest_vertex_batches(g, 0, srcs.data(), starts.data(), sizes.data(), (uint32_t)srcs.size(),
+                                         dsts.data(), dsts.size(), 0, nullptr),
+                "gs_ingest_vertex_batches");
+    srcs.clear();
+    starts.clear();
+    sizes.clear();
+    dsts.clear();
+  }
+
+  node_id_t num_vertices;
+  size_t seed;
+  CCAlgConfiguration config;
+  gs_graph* g = nullptr;
+  std::mutex mtx;
+  bool update_locked = false;
+  size_t flush_at = 1;
+  std::vector<uint32_t> srcs;
+  std::vector<uint64_t> starts, sizes;
+  std::vector<uint32_t> dsts;
+};
+
+// The CPU algorithm's name maps to the same device implementation.
+using CCSketchAlg = CCGPUSketchAlg;

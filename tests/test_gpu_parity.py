@@ -267,7 +267,8 @@ def test_reference_named_api(restatement, golden_dir):
     assert cc.size() == 78
     ids = {frozenset(s) for s in cc.get_component_sets()}
     assert frozenset({2, 4, 6}) <= next(s for s in ids if 2 in s)
-    assert alg.point_query(3, 9) and not alg.point_query(3, 5)
+    # 3-6-2-10-5 joins 3 and 5; a prime p > 511 has no multiple below 1024 and stays alone
+    assert alg.point_query(3, 9) and alg.point_query(3, 5) and not alg.point_query(3, 521)
 
 
 def test_full_size_rmat_properties(restatement, torch_cuda):
