@@ -33,7 +33,7 @@ void free_graph(gs_graph* g) {
   if (!g) return;
   cudaFree(g->d_sk); cudaFree(g->d_colmix);
   cudaFree(g->d_cnt); cudaFree(g->d_off); cudaFree(g->d_choff); cudaFree(g->d_tile);
-  cudaFree(g->d_nbr); cudaFree(g->d_pairs);
+  cudaFree(g->d_nbr); cudaFree(g->d_pairs); cudaFree(g->d_part); cudaFree(g->d_bkt);
   if (g->h_pin) cudaFreeHost(g->h_pin);
   if (g->h_status) cudaFreeHost(g->h_status);
   cudaFree(g->d_status);

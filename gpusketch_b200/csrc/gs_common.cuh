@@ -42,6 +42,23 @@ GS_HD uint64_t gs_mix(uint64_t z) { return z ^ gs_rotl64(z, 49) ^ gs_rotl64(z, 2
 // mix(k') for key k
 GS_HD uint64_t gs_key_mix(uint64_t key) { return gs_mix((key >> 32) | (key << 32)); }
 
+// Inverse of gs_mix.  mix is the GF(2)-linear map M = I + R^49 + R^24 (R = rotate left by one);
+// squaring commuting terms gives M^(2^k) = I + R^(49*2^k) + R^(24*2^k), so M^8 = R^8, M^16 = R^16,
+// M^32 = R^32, M^64 = I and M^-1 = M^63 = M * M^2 * M^4 * R^56.
+GS_HD uint64_t gs_mix_inv(uint64_t z) {
+  z = z ^ gs_rotl64(z, 49) ^ gs_rotl64(z, 24);
+  z = z ^ gs_rotl64(z, 34) ^ gs_rotl64(z, 48);
+  z = z ^ gs_rotl64(z, 4) ^ gs_rotl64(z, 32);
+  return gs_rotl64(z, 56);
+}
+
+// key k from gs_key_mix(k); both maps are XOR-linear, so a XOR of mixed keys unmixes to the XOR
+// of the keys
+GS_HD uint64_t gs_key_unmix(uint64_t mixed) {
+  const uint64_t k = gs_mix_inv(mixed);
+  return (k >> 32) | (k << 32);
+}
+
 // mix(B(seed)) for seed s
 GS_HD uint64_t gs_seed_mix(uint64_t seed) {
   uint32_t lo = (uint32_t)seed;

@@ -31,28 +31,11 @@ namespace {
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
 constexpr int kScanTile = kScanThreads * kScanPer;
-constexpr int kSlabDepth = 8;      // depths cached in shared memory per column
+constexpr int kRegDepth = 3;       // depths [0, 3) of a lane's column live in registers (87.5% of updates)
+constexpr int kSlabDepth = 10;     // depths [3, 10) in a lane-private shared-memory row
 constexpr int kSlabPitch = 33;     // 32 lanes + 1 pad: rows land on distinct bank groups
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
-
-// lanes of `peers` holding the same key combine their increments; returns the old counter value
-// plus this lane's rank among its peers.
-__device__ __forceinline__ uint32_t agg_fetch_add(uint32_t* ctr, uint32_t key, bool act) {
-  const uint32_t lane = lane_id();
-  uint32_t peers = __match_any_sync(0xffffffffu, act ? key : 0xffffffffu);
-  uint32_t leader = __ffs(peers) - 1;
-  uint32_t base = 0;
-  if (act && lane == leader) base = atomicAdd(&ctr[key], (uint32_t)__popc(peers));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return base + __popc(peers & ((1u << lane) - 1u));
-}
-
-__device__ __forceinline__ void agg_add(uint32_t* ctr, uint32_t key, bool act) {
-  const uint32_t lane = lane_id();
-  uint32_t peers = __match_any_sync(0xffffffffu, act ? key : 0xffffffffu);
-  if (act && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&ctr[key], (uint32_t)__popc(peers));
-}
 
 struct PairTag {
   uint32_t V, num_levels, L;
@@ -84,56 +67,222 @@ __device__ __forceinline__ bool record_levels(const PairTag& t, uint32_t u, uint
   return true;
 }
 
-__global__ void k_count_pairs(const uint2* __restrict__ pairs, uint64_t n, PairTag t,
-                              uint32_t* __restrict__ cnt, uint32_t* __restrict__ status) {
-  const uint64_t warp0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t base = warp0 * 32; base < n; base += nwarps * 32) {
-    uint64_t i = base + lane_id();
-    int lo = 0, hi = -1;
-    uint32_t u = 0, v = 0;
-    if (i < n) {
-      uint2 p = pairs[i];
-      u = p.x; v = p.y;
-      if (!record_levels(t, u, v, &lo, &hi, status)) { lo = 0; hi = -1; }
+// ---- exclusive scan of (count, ceil(count/chunk)) over nv entries, totals at [nv] ----
+
+__device__ __forceinline__ uint2 add2(uint2 a, uint2 b) { return make_uint2(a.x + b.x, a.y + b.y); }
+
+__device__ uint2 block_exclusive_scan(uint2 x, uint2* total) {
+  __shared__ uint2 warp_sums[32];
+  __shared__ uint2 block_total;
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  uint2 inc = x;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t a = __shfl_up_sync(0xffffffffu, inc.x, o), b = __shfl_up_sync(0xffffffffu, inc.y, o);
+    if (lane >= (uint32_t)o) { inc.x += a; inc.y += b; }
+  }
+  if (lane == 31) warp_sums[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t nw = blockDim.x >> 5;
+    uint2 s = lane < nw ? warp_sums[lane] : make_uint2(0, 0);
+    uint2 si = s;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t a = __shfl_up_sync(0xffffffffu, si.x, o), b = __shfl_up_sync(0xffffffffu, si.y, o);
+      if (lane >= (uint32_t)o) { si.x += a; si.y += b; }
     }
-    int wlo = __reduce_min_sync(0xffffffffu, hi >= lo ? lo : 0x7fffffff);
-    int whi = __reduce_max_sync(0xffffffffu, hi);
-    for (int g = wlo; g <= whi; g++) {
-      bool act = g >= lo && g <= hi;
-      agg_add(cnt, (uint32_t)g * t.V + u, act);
-      agg_add(cnt, (uint32_t)g * t.V + v, act);
+    if (lane < nw) warp_sums[lane] = make_uint2(si.x - s.x, si.y - s.y);
+    if (lane == nw - 1) block_total = si;  // nw <= 32
+  }
+  __syncthreads();
+  uint2 res = add2(warp_sums[w], make_uint2(inc.x - x.x, inc.y - x.y));
+  *total = block_total;
+  __syncthreads();
+  return res;
+}
+
+// ---- two-level counting sort of the records by virtual vertex ----
+//
+// Pass 1 partitions the records by the high bits of their key (key >> LB, at most kMaxBuckets
+// buckets), pass 2 counts and places them by vertex inside each bucket.  Every histogram lives in
+// shared memory; global atomics happen once per (block, non-empty bucket) and once per (block,
+// non-empty vertex), so hub vertices of skewed streams cost no more than any other vertex.
+
+constexpr int kPartThreads = 512;
+constexpr int kPartEdges = 4096;      // edges per block in pass 1
+constexpr int kVertChunk = 8192;      // partitioned records per block iteration in pass 2
+constexpr int kMaxBuckets = 4096;
+
+__global__ void __launch_bounds__(kPartThreads) k_part_count(const uint2* __restrict__ pairs, uint64_t n, PairTag t,
+                                                             uint32_t lb, uint32_t H, uint32_t* __restrict__ tot,
+                                                             uint32_t* __restrict__ status) {
+  extern __shared__ uint32_t hist[];
+  for (uint32_t i = threadIdx.x; i < H; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const uint64_t e0 = (uint64_t)blockIdx.x * kPartEdges;
+  const uint64_t e1 = min(n, e0 + kPartEdges);
+  for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const uint2 p = pairs[e];
+    int lo = 0, hi = -1;
+    if (!record_levels(t, p.x, p.y, &lo, &hi, status)) continue;
+    for (int g = lo; g <= hi; g++) {
+      atomicAdd(&hist[((uint32_t)g * t.V + p.x) >> lb], 1u);
+      atomicAdd(&hist[((uint32_t)g * t.V + p.y) >> lb], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t d = threadIdx.x; d < H; d += blockDim.x)
+    if (hist[d]) atomicAdd(&tot[d], hist[d]);
+}
+
+// bkt layout: tot[H] | off[H+1] | cur[H] | choff[H+1]; status[1] = records, status[5] = pass-2 chunks
+__global__ void __launch_bounds__(kScanThreads) k_part_scan(uint32_t* __restrict__ bkt, uint32_t H,
+                                                            uint32_t* __restrict__ status) {
+  uint32_t* tot = bkt;
+  uint32_t* off = bkt + H;
+  uint32_t* cur = off + H + 1;
+  uint32_t* choff = cur + H;
+  uint2 carry = make_uint2(0, 0);
+  for (uint32_t b0 = 0; b0 < H; b0 += kScanThreads) {
+    const uint32_t d = b0 + threadIdx.x;
+    const uint32_t c = d < H ? tot[d] : 0u;
+    const uint2 x = make_uint2(c, (c + kVertChunk - 1) / kVertChunk);
+    uint2 total;
+    const uint2 ex = block_exclusive_scan(x, &total);
+    if (d < H) {
+      off[d] = ex.x + carry.x;
+      cur[d] = ex.x + carry.x;
+      choff[d] = ex.y + carry.y;
+    }
+    carry = add2(carry, total);
+  }
+  if (threadIdx.x == 0) {
+    off[H] = carry.x;
+    choff[H] = carry.y;
+    status[1] = carry.x;
+    status[5] = carry.y;
+  }
+}
+
+__global__ void __launch_bounds__(kPartThreads) k_part_scatter(const uint2* __restrict__ pairs, uint64_t n, PairTag t,
+                                                               uint32_t lb, uint32_t H, uint32_t* __restrict__ bkt,
+                                                               uint2* __restrict__ part, uint64_t cap,
+                                                               uint32_t* __restrict__ status) {
+  extern __shared__ uint32_t sh[];
+  uint32_t* hist = sh;
+  uint32_t* base = sh + H;
+  uint32_t* cur = bkt + 2 * H + 1;
+  for (uint32_t i = threadIdx.x; i < H; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const uint64_t e0 = (uint64_t)blockIdx.x * kPartEdges;
+  const uint64_t e1 = min(n, e0 + kPartEdges);
+  PairTag quiet = t;
+  for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const uint2 p = pairs[e];
+    if (p.x >= t.V || p.y >= t.V) continue;  // reported by k_part_count
+    int lo = 0, hi = -1;
+    if (!record_levels(quiet, p.x, p.y, &lo, &hi, status)) continue;
+    for (int g = lo; g <= hi; g++) {
+      atomicAdd(&hist[((uint32_t)g * t.V + p.x) >> lb], 1u);
+      atomicAdd(&hist[((uint32_t)g * t.V + p.y) >> lb], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t d = threadIdx.x; d < H; d += blockDim.x) {
+    const uint32_t c = hist[d];
+    base[d] = c ? atomicAdd(&cur[d], c) : 0u;
+    hist[d] = 0;
+  }
+  __syncthreads();
+  for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const uint2 p = pairs[e];
+    if (p.x >= t.V || p.y >= t.V) continue;
+    int lo = 0, hi = -1;
+    if (!record_levels(quiet, p.x, p.y, &lo, &hi, status)) continue;
+    for (int g = lo; g <= hi; g++) {
+      const uint32_t ku = (uint32_t)g * t.V + p.x, kv = (uint32_t)g * t.V + p.y;
+      const uint32_t pu = base[ku >> lb] + atomicAdd(&hist[ku >> lb], 1u);
+      const uint32_t pv = base[kv >> lb] + atomicAdd(&hist[kv >> lb], 1u);
+      if (pu < cap && pv < cap) {
+        part[pu] = make_uint2(ku, p.y);
+        part[pv] = make_uint2(kv, p.x);
+      } else {
+        atomicOr(status, (uint32_t)GS_DEV_ERR_CAPACITY);
+      }
     }
   }
 }
 
-__global__ void k_scatter_pairs(const uint2* __restrict__ pairs, uint64_t n, PairTag t,
-                                uint32_t* __restrict__ cursor, uint32_t* __restrict__ nbr,
-                                uint64_t cap, uint32_t* __restrict__ status) {
-  const uint64_t warp0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t base = warp0 * 32; base < n; base += nwarps * 32) {
-    uint64_t i = base + lane_id();
-    int lo = 0, hi = -1;
-    uint32_t u = 0, v = 0;
-    if (i < n) {
-      uint2 p = pairs[i];
-      u = p.x; v = p.y;
-      // range errors were already reported by the count pass
-      if (u >= t.V || v >= t.V || u == v) { hi = -1; }
-      else if (!record_levels(t, u, v, &lo, &hi, status)) { lo = 0; hi = -1; }
+// the bucket of pass-2 chunk c: largest d with choff[d] <= c
+__device__ __forceinline__ uint32_t chunk_bucket(const uint32_t* choff, uint32_t H, uint32_t c) {
+  uint32_t lo = 0, hi = H;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (choff[mid] <= c) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// pass 2, counting: records per vertex of each bucket chunk
+__global__ void __launch_bounds__(kPartThreads) k_vert_count(const uint2* __restrict__ part, const uint32_t* __restrict__ bkt,
+                                                             uint32_t H, uint32_t lb, uint32_t* __restrict__ cnt,
+                                                             const uint32_t* __restrict__ status) {
+  extern __shared__ uint32_t hist[];
+  __shared__ uint32_t s_d;
+  const uint32_t* off = bkt + H;
+  const uint32_t* choff = bkt + 3 * H + 1;
+  const uint32_t nk = 1u << lb, mask = nk - 1;
+  const uint32_t total = status[5];
+  for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+    if (threadIdx.x == 0) s_d = chunk_bucket(choff, H, c);
+    for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const uint32_t d = s_d;
+    const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
+    const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&hist[part[i].x & mask], 1u);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nk; k += blockDim.x)
+      if (hist[k]) atomicAdd(&cnt[(d << lb) + k], hist[k]);
+    __syncthreads();
+  }
+}
+
+// pass 2, placement: each record's neighbour goes to its vertex's slice of nbr
+__global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __restrict__ part, const uint32_t* __restrict__ bkt,
+                                                               uint32_t H, uint32_t lb, uint32_t* __restrict__ cursor,
+                                                               uint32_t* __restrict__ nbr, uint64_t cap,
+                                                               uint32_t* __restrict__ status) {
+  extern __shared__ uint32_t sh[];
+  __shared__ uint32_t s_d;
+  const uint32_t nk = 1u << lb, mask = nk - 1;
+  uint32_t* hist = sh;
+  uint32_t* base = sh + nk;
+  const uint32_t* off = bkt + H;
+  const uint32_t* choff = bkt + 3 * H + 1;
+  const uint32_t total = status[5];
+  for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+    if (threadIdx.x == 0) s_d = chunk_bucket(choff, H, c);
+    for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const uint32_t d = s_d;
+    const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
+    const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&hist[part[i].x & mask], 1u);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < nk; k += blockDim.x) {
+      const uint32_t h = hist[k];
+      base[k] = h ? atomicAdd(&cursor[(d << lb) + k], h) : 0u;
+      hist[k] = 0;
     }
-    int wlo = __reduce_min_sync(0xffffffffu, hi >= lo ? lo : 0x7fffffff);
-    int whi = __reduce_max_sync(0xffffffffu, hi);
-    for (int g = wlo; g <= whi; g++) {
-      bool act = g >= lo && g <= hi;
-      uint32_t pu = agg_fetch_add(cursor, (uint32_t)g * t.V + u, act);
-      uint32_t pv = agg_fetch_add(cursor, (uint32_t)g * t.V + v, act);
-      if (act) {
-        if (pu < cap && pv < cap) { nbr[pu] = v; nbr[pv] = u; }
-        else atomicOr(status, (uint32_t)GS_DEV_ERR_CAPACITY);
-      }
+    __syncthreads();
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const uint2 r = part[i];
+      const uint32_t k = r.x & mask;
+      const uint32_t pos = base[k] + atomicAdd(&hist[k], 1u);
+      if (pos < cap) nbr[pos] = r.y;
+      else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
     }
+    __syncthreads();
   }
 }
 
@@ -170,39 +319,6 @@ __global__ void k_scatter_batches(const uint32_t* __restrict__ srcs, const uint6
       else atomicOr(status, (uint32_t)GS_DEV_ERR_CAPACITY);
     }
   }
-}
-
-// ---- exclusive scan of (count, ceil(count/chunk)) over nv entries, totals at [nv] ----
-
-__device__ __forceinline__ uint2 add2(uint2 a, uint2 b) { return make_uint2(a.x + b.x, a.y + b.y); }
-
-__device__ uint2 block_exclusive_scan(uint2 x, uint2* total) {
-  __shared__ uint2 warp_sums[32];
-  __shared__ uint2 block_total;
-  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-  uint2 inc = x;
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t a = __shfl_up_sync(0xffffffffu, inc.x, o), b = __shfl_up_sync(0xffffffffu, inc.y, o);
-    if (lane >= (uint32_t)o) { inc.x += a; inc.y += b; }
-  }
-  if (lane == 31) warp_sums[w] = inc;
-  __syncthreads();
-  if (w == 0) {
-    uint32_t nw = blockDim.x >> 5;
-    uint2 s = lane < nw ? warp_sums[lane] : make_uint2(0, 0);
-    uint2 si = s;
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t a = __shfl_up_sync(0xffffffffu, si.x, o), b = __shfl_up_sync(0xffffffffu, si.y, o);
-      if (lane >= (uint32_t)o) { si.x += a; si.y += b; }
-    }
-    if (lane < nw) warp_sums[lane] = make_uint2(si.x - s.x, si.y - s.y);
-    if (lane == nw - 1) block_total = si;  // nw <= 32
-  }
-  __syncthreads();
-  uint2 res = add2(warp_sums[w], make_uint2(inc.x - x.x, inc.y - x.y));
-  *total = block_total;
-  __syncthreads();
-  return res;
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ cnt, uint32_t nv,
@@ -287,21 +403,26 @@ __device__ __forceinline__ void xor_bucket_global(GsBucket* p, uint64_t a, uint6
   atomicXor(reinterpret_cast<unsigned long long*>(&p->gamma), (unsigned long long)g);
 }
 
+// Per lane: buckets of depth < kRegDepth of its column(s) in registers, depth [kRegDepth, kSlabDepth)
+// in a lane-private shared-memory row, deeper ones straight into HBM.  Buckets accumulate
+// {mix(k'), checksum} instead of {edge id, checksum}: gs_key_mix is XOR-linear, so XOR-ing mixed
+// keys and unmixing once per bucket at merge time (gs_key_unmix) gives the XOR of the edge ids, and
+// every record is a single 16-byte broadcast {mix(k'), checksum}.
 template <int CG>
 __global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
   extern __shared__ uint4 smem[];
-  constexpr int kSlabWords = CG * kSlabDepth * kSlabPitch;  // uint4 per warp slab
+  constexpr int kRows = kSlabDepth - kRegDepth;
+  constexpr int kSlabWords = CG * kRows * kSlabPitch;  // uint4 per warp slab
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
-  uint4* slab = smem + (size_t)wib * (kSlabWords + 32 + 16);
-  uint4* rec = slab + kSlabWords;                              // 32 x {mix(k') , checksum}
-  uint2* rec_e = reinterpret_cast<uint2*>(rec + 32);           // 32 x edge id
+  uint4* slab = smem + (size_t)wib * (kSlabWords + 32);
+  uint4* rec = slab + kSlabWords;                     // 32 x {mix(k'), checksum}
 
   const uint32_t C = A.C, bkt = A.bkt, nb = A.nb, V = A.V;
   const uint64_t csmix = A.colmix[C];
   uint64_t cmix[CG];
 #pragma unroll
   for (int g = 0; g < CG; g++) {
-    uint32_t c = lane + 32u * g;
+    const uint32_t c = lane + 32u * g;
     cmix[g] = c < C ? A.colmix[c] : 0ull;
   }
 
@@ -313,10 +434,10 @@ __global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
     // owner vertex: the largest vv with choff[vv] <= ch (32-way search across the warp)
     uint32_t lo = 0, hi = A.nv;
     while (hi - lo > 1) {
-      uint32_t step = (hi - lo + 31) / 32;
-      uint32_t probe = lo + (lane + 1) * step;
-      bool le = probe < hi && A.choff[probe] <= ch;
-      uint32_t k = __popc(__ballot_sync(0xffffffffu, le));
+      const uint32_t step = (hi - lo + 31) / 32;
+      const uint32_t probe = lo + (lane + 1) * step;
+      const bool le = probe < hi && A.choff[probe] <= ch;
+      const uint32_t k = __popc(__ballot_sync(0xffffffffu, le));
       lo = lo + k * step;
       hi = min(hi, lo + step);
     }
@@ -329,38 +450,47 @@ __global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
     GsBucket* skv = A.sk + (size_t)vv * nb;
 
     for (int i = lane; i < kSlabWords; i += 32) slab[i] = make_uint4(0, 0, 0, 0);
-    uint64_t det_a = 0, det_g = 0;
+    uint4 acc[CG][kRegDepth];
+#pragma unroll
+    for (int g = 0; g < CG; g++)
+#pragma unroll
+      for (int d = 0; d < kRegDepth; d++) acc[g][d] = make_uint4(0, 0, 0, 0);
+    uint64_t det_m = 0, det_g = 0;
     __syncwarp();
 
     for (uint32_t b = rb; b < re; b += 32) {
       const uint32_t r = b + lane;
       const bool valid = r < re;
       const uint32_t u = valid ? A.nbr[r] : v;
-      const uint64_t e = gs_concat(v, u);
-      const uint64_t E = gs_key_mix(e);
+      const uint64_t E = gs_key_mix(gs_concat(v, u));
       const uint64_t cs = gs_hash_tail(E ^ csmix);
-      if (valid) { det_a ^= e; det_g ^= cs; }
+      if (valid) { det_m ^= E; det_g ^= cs; }
       rec[lane] = make_uint4((uint32_t)E, (uint32_t)(E >> 32), (uint32_t)cs, (uint32_t)(cs >> 32));
-      rec_e[lane] = make_uint2((uint32_t)e, (uint32_t)(e >> 32));
       __syncwarp();
       const uint32_t cnt = min(32u, re - b);
       for (uint32_t j = 0; j < cnt; j++) {
         const uint4 q = rec[j];
-        const uint2 qe = rec_e[j];
         const uint64_t Ej = ((uint64_t)q.y << 32) | q.x;
 #pragma unroll
         for (int g = 0; g < CG; g++) {
           const uint32_t c = lane + 32u * g;
           if (c < C) {
             const uint32_t d = gs_depth_from_mixed(Ej ^ cmix[g], bkt);
-            if (d < (uint32_t)kSlabDepth) {
-              uint4* p = slab + (g * kSlabDepth + d) * kSlabPitch + lane;
-              uint4 t = *p;
-              t.x ^= qe.x; t.y ^= qe.y; t.z ^= q.z; t.w ^= q.w;
-              *p = t;
-            } else if (d < bkt) {
-              xor_bucket_global(skv + (size_t)c * bkt + d, ((uint64_t)qe.y << 32) | qe.x,
-                                ((uint64_t)q.w << 32) | q.z);
+#pragma unroll
+            for (int k = 0; k < kRegDepth; k++) {
+              if (d == (uint32_t)k) {
+                acc[g][k].x ^= q.x; acc[g][k].y ^= q.y; acc[g][k].z ^= q.z; acc[g][k].w ^= q.w;
+              }
+            }
+            if (d >= (uint32_t)kRegDepth) {
+              if (d < (uint32_t)kSlabDepth) {
+                uint4* p = slab + (g * kRows + (d - kRegDepth)) * kSlabPitch + lane;
+                uint4 t = *p;
+                t.x ^= q.x; t.y ^= q.y; t.z ^= q.z; t.w ^= q.w;
+                *p = t;
+              } else if (d < bkt) {
+                xor_bucket_global(skv + (size_t)c * bkt + d, gs_key_unmix(Ej), ((uint64_t)q.w << 32) | q.z);
+              }
             }
           }
         }
@@ -368,45 +498,55 @@ __global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
       __syncwarp();
     }
 
-    // merge the slab: item i -> column i / D, depth i % D, so 8 consecutive lanes cover one
-    // column's 128 contiguous bytes
+    // merge the register depths: lane c owns the first kRegDepth buckets of column c
+#pragma unroll
+    for (int g = 0; g < CG; g++) {
+      const uint32_t c = lane + 32u * g;
+      if (c >= C) continue;
+#pragma unroll
+      for (int d = 0; d < kRegDepth; d++) {
+        const uint4 t = acc[g][d];
+        if ((t.x | t.y | t.z | t.w) == 0u) continue;
+        const uint64_t a = gs_key_unmix(((uint64_t)t.y << 32) | t.x), gm = ((uint64_t)t.w << 32) | t.z;
+        GsBucket* p = skv + (size_t)c * bkt + d;
+        if (exclusive) { p->alpha ^= a; p->gamma ^= gm; }
+        else xor_bucket_global(p, a, gm);
+      }
+    }
+    __syncwarp();
+    // merge the slab rows: item i -> column i / kRows, depth kRegDepth + i % kRows, so consecutive lanes
+    // cover contiguous buckets of one column
 #pragma unroll
     for (int g = 0; g < CG; g++) {
       const uint32_t cols = min(32u, C - min(C, 32u * g));
-      for (uint32_t i = lane; i < cols * kSlabDepth; i += 32) {
-        const uint32_t cl = i / kSlabDepth, d = i % kSlabDepth;
-        if (d >= bkt) continue;
-        const uint4 t = slab[(g * kSlabDepth + d) * kSlabPitch + cl];
+      for (uint32_t i = lane; i < cols * kRows; i += 32) {
+        const uint32_t cl = i / kRows, row = i % kRows;
+        const uint4 t = slab[(g * kRows + row) * kSlabPitch + cl];
         if ((t.x | t.y | t.z | t.w) == 0u) continue;
-        GsBucket* p = skv + (size_t)(cl + 32u * g) * bkt + d;
-        const uint64_t a = ((uint64_t)t.y << 32) | t.x, gm = ((uint64_t)t.w << 32) | t.z;
-        if (exclusive) {
-          uint4* q4 = reinterpret_cast<uint4*>(p);
-          uint4 o = *q4;
-          o.x ^= t.x; o.y ^= t.y; o.z ^= t.z; o.w ^= t.w;
-          *q4 = o;
-        } else {
-          xor_bucket_global(p, a, gm);
-        }
+        const uint64_t a = gs_key_unmix(((uint64_t)t.y << 32) | t.x), gm = ((uint64_t)t.w << 32) | t.z;
+        GsBucket* p = skv + (size_t)(cl + 32u * g) * bkt + kRegDepth + row;
+        if (exclusive) { p->alpha ^= a; p->gamma ^= gm; }
+        else xor_bucket_global(p, a, gm);
       }
     }
     // deterministic bucket (last bucket of the sketch)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      det_a ^= __shfl_xor_sync(0xffffffffu, det_a, o);
+      det_m ^= __shfl_xor_sync(0xffffffffu, det_m, o);
       det_g ^= __shfl_xor_sync(0xffffffffu, det_g, o);
     }
-    if (lane == 0 && (det_a | det_g) != 0ull) {
+    if (lane == 0 && (det_m | det_g) != 0ull) {
       GsBucket* p = skv + (nb - 1);
-      if (exclusive) { p->alpha ^= det_a; p->gamma ^= det_g; }
-      else xor_bucket_global(p, det_a, det_g);
+      const uint64_t a = gs_key_unmix(det_m);
+      if (exclusive) { p->alpha ^= a; p->gamma ^= det_g; }
+      else xor_bucket_global(p, a, det_g);
     }
     __syncwarp();
   }
 }
 
 size_t ingest_smem_bytes(int cg, int warps) {
-  return (size_t)warps * (size_t)(cg * kSlabDepth * kSlabPitch + 32 + 16) * sizeof(uint4);
+  return (size_t)warps * (size_t)(cg * (kSlabDepth - kRegDepth) * kSlabPitch + 32) * sizeof(uint4);
 }
 
 template <int CG>
@@ -417,13 +557,22 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   A.bkt = g->geom.bkt_per_col; A.nb = g->geom.num_buckets; A.chunk = g->tune.chunk;
   const int warps = (int)g->tune.warps_per_block;
   const size_t smem = ingest_smem_bytes(CG, warps);
-  // the opt-in shared-memory limit is a per-device function attribute
+  // the opt-in shared-memory limit is a per-device function attribute; the persistent grid fills
+  // every SM with as many blocks as registers and shared memory allow
   static size_t attr_bytes[64][2] = {};
-  if (g->device < 64 && attr_bytes[g->device][CG - 1] < smem) {
+  static int occ_blocks[64][2] = {};
+  const int dev = g->device < 64 ? g->device : 63;
+  if (attr_bytes[dev][CG - 1] < smem) {
     GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest<CG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_bytes[g->device][CG - 1] = smem;
+    attr_bytes[dev][CG - 1] = smem;
+    occ_blocks[dev][CG - 1] = 0;
   }
-  const int blocks = g->num_sms * (int)g->tune.blocks_per_sm;
+  if (occ_blocks[dev][CG - 1] == 0) {
+    int nb = 0;
+    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG>, warps * 32, smem));
+    occ_blocks[dev][CG - 1] = nb > 0 ? nb : 1;
+  }
+  const int blocks = g->num_sms * occ_blocks[dev][CG - 1];
   k_ingest<CG><<<blocks, warps * 32, smem, s>>>(A);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
@@ -449,6 +598,26 @@ gs_status gs_ensure_ingest_scratch(gs_graph* g, uint64_t records) {
     g->nbr_cap = 0;
     GS_CUDA_TRY(cudaMalloc(&g->d_nbr, records * sizeof(uint32_t)));
     g->nbr_cap = records;
+  }
+  return GS_OK;
+}
+
+// records partitioned by key bucket (pass 1 output) and the bucket tables
+static gs_status ensure_partition_scratch(gs_graph* g, uint64_t records) {
+  const uint64_t nv = (uint64_t)g->num_levels * g->V;
+  if (!g->d_bkt) {
+    uint32_t lb = 9;
+    while ((nv >> lb) >= (uint64_t)kMaxBuckets) lb++;
+    g->part_lb = lb;
+    g->part_buckets = (uint32_t)((nv + (1ull << lb) - 1) >> lb);
+    GS_CUDA_TRY(cudaMalloc(&g->d_bkt, (4 * (size_t)g->part_buckets + 2) * sizeof(uint32_t)));
+  }
+  if (g->part_cap < records) {
+    cudaFree(g->d_part);
+    g->d_part = nullptr;
+    g->part_cap = 0;
+    GS_CUDA_TRY(cudaMalloc(&g->d_part, records * sizeof(uint2)));
+    g->part_cap = records;
   }
   return GS_OK;
 }
@@ -487,25 +656,37 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
   for (uint64_t done = 0; done < n;) {
     const uint64_t m = std::min<uint64_t>(n - done, g->max_batch_edges);
     const uint2* p = reinterpret_cast<const uint2*>(d_pairs) + done;
-    GS_TRY(gs_ensure_ingest_scratch(g, tagged ? g->nbr_cap : 2 * m));
-    GS_CUDA_TRY(cudaMemsetAsync(g->d_cnt, 0, (size_t)(nv + 1) * sizeof(uint32_t), s));
-    const int grid = grid_for(g, m, 256);
+    const uint64_t bound = tagged ? std::max<uint64_t>(g->part_cap, 4 * m) : 2 * m;
+    GS_TRY(gs_ensure_ingest_scratch(g, tagged ? std::max<uint64_t>(g->nbr_cap, 4 * m) : 2 * m));
+    GS_TRY(ensure_partition_scratch(g, bound));
+    const uint32_t H = g->part_buckets, lb = g->part_lb;
+    const unsigned tiles = (unsigned)((m + kPartEdges - 1) / kPartEdges);
+    const int grid2 = g->num_sms * 4;
     {
-      GsProfScope ps(g, GS_PROF_BUCKET, s, 4);
-      k_count_pairs<<<grid, 256, 0, s>>>(p, m, t, g->d_cnt, g->d_status);
+      GsProfScope ps(g, GS_PROF_BUCKET, s, 2);
+      GS_CUDA_TRY(cudaMemsetAsync(g->d_bkt, 0, (size_t)H * sizeof(uint32_t), s));
+      GS_CUDA_TRY(cudaMemsetAsync(g->d_cnt, 0, (size_t)(nv + 1) * sizeof(uint32_t), s));
+      k_part_count<<<tiles, kPartThreads, H * sizeof(uint32_t), s>>>(p, m, t, lb, H, g->d_bkt, g->d_status);
+      k_part_scan<<<1, kScanThreads, 0, s>>>(g->d_bkt, H, g->d_status);
       GS_CUDA_TRY(cudaGetLastError());
-      GS_TRY(scan_counts(g, nv, s));
     }
     if (tagged) {
-      // record count depends on the tags: read it back and grow the scratch if needed
-      GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      // the record count depends on the tags: read it back and grow the scratch if needed
+      GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       GS_CUDA_TRY(cudaStreamSynchronize(s));
-      uint64_t recs = g->h_status[1];
+      const uint64_t recs = g->h_status[1];
+      if (recs > g->part_cap) GS_TRY(ensure_partition_scratch(g, recs + recs / 8));
       if (recs > g->nbr_cap) GS_TRY(gs_ensure_ingest_scratch(g, recs + recs / 8));
     }
     {
-      GsProfScope ps(g, GS_PROF_BUCKET, s, 1);
-      k_scatter_pairs<<<grid, 256, 0, s>>>(p, m, t, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status);
+      GsProfScope ps(g, GS_PROF_BUCKET, s, 6);
+      k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, m, t, lb, H, g->d_bkt, g->d_part,
+                                                                           g->part_cap, g->d_status);
+      k_vert_count<<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt,
+                                                                             g->d_status);
+      GS_TRY(scan_counts(g, nv, s));
+      k_vert_scatter<<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(
+          g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status);
       GS_CUDA_TRY(cudaGetLastError());
     }
     {

@@ -43,13 +43,18 @@ struct gs_graph {
   uint32_t* d_tile = nullptr;  // [2*tiles] per-tile sums for the scan
   uint32_t* d_nbr = nullptr;   // [nbr_cap] neighbour of each record, grouped by virtual vertex
   uint64_t nbr_cap = 0;
+  uint2* d_part = nullptr;     // [part_cap] (key, neighbour) records partitioned by key >> part_lb
+  uint64_t part_cap = 0;
+  uint32_t* d_bkt = nullptr;   // bucket tables of the partition: tot[H] off[H+1] cur[H] choff[H+1]
+  uint32_t part_buckets = 0;   // H
+  uint32_t part_lb = 9;        // low key bits resolved by the second pass
   uint32_t* d_pairs = nullptr; // staging for host-resident input pairs, 2 x [pairs_cap] u32 pairs
   uint64_t pairs_cap = 0;
   void* h_pin = nullptr;       // 2 pinned staging buffers of pairs_cap pairs
   cudaStream_t copy_stream = nullptr;               // H2D of host input slices
   cudaEvent_t ev_copy[2] = {nullptr, nullptr};      // slice copied into d_pairs[slot]
   cudaEvent_t ev_done[2] = {nullptr, nullptr};      // slice in d_pairs[slot] consumed
-  uint32_t* d_status = nullptr;  // [0] error bits [1] records [2] chunks [3] modified [4] count
+  uint32_t* d_status = nullptr;  // [0] error bits [1] records [2] chunks [3] modified [4] forest [5] part chunks
   uint32_t* h_status = nullptr;  // pinned mirror
 
   // ---- Boruvka scratch ----
