@@ -531,6 +531,30 @@ gs_status gs_gen_rmat_stream(uint32_t log2_v, double a, double b, double c, doub
 
 }  // extern "C"
 
+// ---- tuning ----
+
+extern "C" gs_status gs_get_tuning(const gs_graph* g, gs_tuning* out) {
+  if (!g || !out) { gs_set_error("null argument"); return GS_ERR_BAD_ARG; }
+  out->chunk = g->tune.chunk;
+  out->warps_per_block = g->tune.warps_per_block;
+  out->reg_depth = g->tune.reg_depth;
+  out->reserved = 0;
+  return GS_OK;
+}
+
+extern "C" gs_status gs_set_tuning(gs_graph* g, const gs_tuning* t) {
+  if (!g || !t) { gs_set_error("null argument"); return GS_ERR_BAD_ARG; }
+  if (t->chunk < 32 || t->chunk > (1u << 20) || t->warps_per_block < 1 || t->warps_per_block > 16 ||
+      t->reg_depth < 1 || t->reg_depth > 3) {
+    gs_set_error("gs_set_tuning: chunk in [32, 2^20], warps_per_block in [1, 16], reg_depth in [1, 3]");
+    return GS_ERR_BAD_ARG;
+  }
+  g->tune.chunk = t->chunk;
+  g->tune.warps_per_block = t->warps_per_block;
+  g->tune.reg_depth = t->reg_depth;
+  return GS_OK;
+}
+
 // ---- profiling ----
 
 GsProfScope::GsProfScope(gs_graph* g_, int cls_, cudaStream_t s_, uint32_t launches) : g(g_), cls(cls_), s(s_) {

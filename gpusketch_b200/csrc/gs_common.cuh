@@ -93,18 +93,21 @@ GS_HD uint64_t gs_concat(uint32_t a, uint32_t b) {
 // (Bucket_Boruvka::get_index_depth, include/bucket.h:54-59).  Computes only the low word of the
 // final xorshift unless it is zero (probability 2^-32).
 __device__ __forceinline__ uint32_t gs_depth_from_mixed(uint64_t x, uint32_t max_depth) {
+  // the shifts are written as multiplies so they issue on the FMA pipe, next to the 64-bit
+  // products, instead of the ALU pipe that carries the XORs: (hi >> 3) = umulhi(hi, 2^29),
+  // (h2:l2) >> 28 = (h2 << 4) | (l2 >> 28) = h2 * 16 ^ umulhi(l2, 16)
   uint64_t h = x * kGsMx2;
   uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
-  lo ^= (hi >> 3) + 8u;
+  lo ^= __umulhi(hi, 1u << 29) + 8u;
   h = ((uint64_t)hi << 32) | lo;
   h *= kGsMx2;
-  uint32_t l2 = (uint32_t)h, h2 = (uint32_t)(h >> 32);
-  uint32_t flo = l2 ^ __funnelshift_r(l2, h2, 28);
+  const uint32_t l2 = (uint32_t)h, h2 = (uint32_t)(h >> 32);
+  const uint32_t flo = l2 ^ (h2 * 16u) ^ __umulhi(l2, 16u);
   uint32_t d;
   if (flo != 0u) {
     d = (uint32_t)(__ffs(flo) - 1);
   } else {
-    uint32_t fhi = h2 ^ (h2 >> 28);
+    const uint32_t fhi = h2 ^ (h2 >> 28);
     d = fhi ? 32u + (uint32_t)(__ffs(fhi) - 1) : 64u;
   }
   return d < max_depth ? d : max_depth;

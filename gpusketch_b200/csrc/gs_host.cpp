@@ -56,7 +56,7 @@ GsTuning gs_tune_for(const GsGeom& geom, int num_sms) {
   GsTuning t;
   t.chunk = 4096;
   t.warps_per_block = 8;
-  t.blocks_per_sm = geom.num_columns <= 32 ? 5 : 2;
+  t.reg_depth = 2;
   return t;
 }
 

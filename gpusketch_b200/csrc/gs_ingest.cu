@@ -31,8 +31,8 @@ namespace {
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
 constexpr int kScanTile = kScanThreads * kScanPer;
-constexpr int kRegDepth = 3;       // depths [0, 3) of a lane's column live in registers (87.5% of updates)
-constexpr int kSlabDepth = 10;     // depths [3, 10) in a lane-private shared-memory row
+constexpr int kMaxRegDepth = 3;    // depths [0, R) of a lane's column live in registers (R <= 3)
+constexpr int kSlabDepth = 10;     // depths [R, 10) in a lane-private shared-memory row
 constexpr int kSlabPitch = 33;     // 32 lanes + 1 pad: rows land on distinct bank groups
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -408,9 +408,12 @@ __device__ __forceinline__ void xor_bucket_global(GsBucket* p, uint64_t a, uint6
 // {mix(k'), checksum} instead of {edge id, checksum}: gs_key_mix is XOR-linear, so XOR-ing mixed
 // keys and unmixing once per bucket at merge time (gs_key_unmix) gives the XOR of the edge ids, and
 // every record is a single 16-byte broadcast {mix(k'), checksum}.
-template <int CG>
-__global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
+// R: depths held in registers.  SMALL: the geometry has bkt_per_col < kSlabDepth (V <= 23), so every
+// path checks the depth against bkt_per_col; otherwise only the rare global path does.
+template <int CG, int R, bool SMALL>
+__global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
   extern __shared__ uint4 smem[];
+  constexpr int kRegDepth = R;
   constexpr int kRows = kSlabDepth - kRegDepth;
   constexpr int kSlabWords = CG * kRows * kSlabPitch;  // uint4 per warp slab
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
@@ -475,14 +478,13 @@ __global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
         for (int g = 0; g < CG; g++) {
           const uint32_t c = lane + 32u * g;
           if (c < C) {
-            const uint32_t d = gs_depth_from_mixed(Ej ^ cmix[g], bkt);
+            const uint32_t d = gs_depth_from_mixed(Ej ^ cmix[g], bkt);  // d == bkt: no bucket
 #pragma unroll
             for (int k = 0; k < kRegDepth; k++) {
-              if (d == (uint32_t)k) {
-                acc[g][k].x ^= q.x; acc[g][k].y ^= q.y; acc[g][k].z ^= q.z; acc[g][k].w ^= q.w;
-              }
+              const bool hit = SMALL ? (d == (uint32_t)k && d < bkt) : d == (uint32_t)k;
+              if (hit) { acc[g][k].x ^= q.x; acc[g][k].y ^= q.y; acc[g][k].z ^= q.z; acc[g][k].w ^= q.w; }
             }
-            if (d >= (uint32_t)kRegDepth) {
+            if (d >= (uint32_t)kRegDepth && (!SMALL || d < bkt)) {
               if (d < (uint32_t)kSlabDepth) {
                 uint4* p = slab + (g * kRows + (d - kRegDepth)) * kSlabPitch + lane;
                 uint4 t = *p;
@@ -506,7 +508,7 @@ __global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
 #pragma unroll
       for (int d = 0; d < kRegDepth; d++) {
         const uint4 t = acc[g][d];
-        if ((t.x | t.y | t.z | t.w) == 0u) continue;
+        if ((uint32_t)d >= bkt || (t.x | t.y | t.z | t.w) == 0u) continue;
         const uint64_t a = gs_key_unmix(((uint64_t)t.y << 32) | t.x), gm = ((uint64_t)t.w << 32) | t.z;
         GsBucket* p = skv + (size_t)c * bkt + d;
         if (exclusive) { p->alpha ^= a; p->gamma ^= gm; }
@@ -522,7 +524,7 @@ __global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
       for (uint32_t i = lane; i < cols * kRows; i += 32) {
         const uint32_t cl = i / kRows, row = i % kRows;
         const uint4 t = slab[(g * kRows + row) * kSlabPitch + cl];
-        if ((t.x | t.y | t.z | t.w) == 0u) continue;
+        if (kRegDepth + row >= bkt || (t.x | t.y | t.z | t.w) == 0u) continue;
         const uint64_t a = gs_key_unmix(((uint64_t)t.y << 32) | t.x), gm = ((uint64_t)t.w << 32) | t.z;
         GsBucket* p = skv + (size_t)(cl + 32u * g) * bkt + kRegDepth + row;
         if (exclusive) { p->alpha ^= a; p->gamma ^= gm; }
@@ -545,37 +547,43 @@ __global__ void __launch_bounds__(256) k_ingest(const IngestArgs A) {
   }
 }
 
-size_t ingest_smem_bytes(int cg, int warps) {
-  return (size_t)warps * (size_t)(cg * (kSlabDepth - kRegDepth) * kSlabPitch + 32) * sizeof(uint4);
+size_t ingest_smem_bytes(int cg, int r, int warps) {
+  return (size_t)warps * (size_t)(cg * (kSlabDepth - r) * kSlabPitch + 32) * sizeof(uint4);
 }
 
-template <int CG>
+template <int CG, int R, bool SMALL>
 gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   IngestArgs A;
   A.off = g->d_off; A.choff = g->d_choff; A.nbr = g->d_nbr; A.sk = g->d_sk; A.colmix = g->d_colmix;
   A.status = g->d_status; A.nv = nv; A.V = g->V; A.C = g->geom.num_columns;
   A.bkt = g->geom.bkt_per_col; A.nb = g->geom.num_buckets; A.chunk = g->tune.chunk;
   const int warps = (int)g->tune.warps_per_block;
-  const size_t smem = ingest_smem_bytes(CG, warps);
+  const size_t smem = ingest_smem_bytes(CG, R, warps);
   // the opt-in shared-memory limit is a per-device function attribute; the persistent grid fills
   // every SM with as many blocks as registers and shared memory allow
-  static size_t attr_bytes[64][2] = {};
-  static int occ_blocks[64][2] = {};
-  const int dev = g->device < 64 ? g->device : 63;
-  if (attr_bytes[dev][CG - 1] < smem) {
-    GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest<CG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_bytes[dev][CG - 1] = smem;
-    occ_blocks[dev][CG - 1] = 0;
-  }
-  if (occ_blocks[dev][CG - 1] == 0) {
+  struct Cache { size_t smem = 0; int warps = 0; int blocks = 0; };
+  static Cache cache[64];
+  Cache& cc = cache[g->device < 64 ? g->device : 63];
+  if (cc.smem != smem || cc.warps != warps) {
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest<CG, R, SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int nb = 0;
-    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG>, warps * 32, smem));
-    occ_blocks[dev][CG - 1] = nb > 0 ? nb : 1;
+    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, R, SMALL>, warps * 32, smem));
+    cc.smem = smem;
+    cc.warps = warps;
+    cc.blocks = nb > 0 ? nb : 1;
   }
-  const int blocks = g->num_sms * occ_blocks[dev][CG - 1];
-  k_ingest<CG><<<blocks, warps * 32, smem, s>>>(A);
+  k_ingest<CG, R, SMALL><<<g->num_sms * cc.blocks, warps * 32, smem, s>>>(A);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
+}
+
+template <int CG, bool SMALL>
+gs_status launch_ingest_r(gs_graph* g, uint32_t nv, cudaStream_t s) {
+  switch (g->tune.reg_depth) {
+    case 1: return launch_ingest<CG, 1, SMALL>(g, nv, s);
+    case 3: return launch_ingest<CG, 3, SMALL>(g, nv, s);
+    default: return launch_ingest<CG, 2, SMALL>(g, nv, s);
+  }
 }
 
 }  // namespace
@@ -632,8 +640,11 @@ static gs_status scan_counts(gs_graph* g, uint32_t nv, cudaStream_t s) {
 }
 
 static gs_status ingest_chunks(gs_graph* g, uint32_t nv, cudaStream_t s) {
-  if (g->geom.num_columns <= 32) return launch_ingest<1>(g, nv, s);
-  if (g->geom.num_columns <= 64) return launch_ingest<2>(g, nv, s);
+  const bool small = g->geom.bkt_per_col < (uint32_t)kSlabDepth;
+  if (g->geom.num_columns <= 32)
+    return small ? launch_ingest_r<1, true>(g, nv, s) : launch_ingest_r<1, false>(g, nv, s);
+  if (g->geom.num_columns <= 64)
+    return small ? launch_ingest_r<2, true>(g, nv, s) : launch_ingest_r<2, false>(g, nv, s);
   gs_set_error("more than 64 sketch columns are not supported");
   return GS_ERR_BAD_ARG;
 }

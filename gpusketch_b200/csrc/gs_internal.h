@@ -11,7 +11,7 @@
 struct GsTuning {
   uint32_t chunk;            // records per work item; larger vertices are split across warps
   uint32_t warps_per_block;  // warps in an ingest block
-  uint32_t blocks_per_sm;    // resident ingest blocks per SM the grid is sized for
+  uint32_t reg_depth;        // bucket depths each lane keeps in registers (1..3)
 };
 
 struct gs_graph {

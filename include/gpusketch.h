@@ -186,6 +186,19 @@ gs_status gs_upload_sketches(gs_graph* g, uint32_t level, uint32_t first_vertex,
 gs_status gs_write_binary(gs_graph* g, const char* path);
 gs_status gs_read_binary(const char* path, int32_t device, gs_graph** out);
 
+/* ---- tuning (set by the autotuner, gpusketch_b200/autotune.py) ---- */
+typedef struct gs_tuning {
+  uint32_t chunk;            /* records per sketch-update work item (>= 32) */
+  uint32_t warps_per_block;  /* warps per sketch-update block (1..16) */
+  uint32_t reg_depth;        /* bucket depths each lane keeps in registers (1..3) */
+  uint32_t reserved;
+} gs_tuning;
+/* Reads / replaces the launch parameters of the sketch-update kernel.  Results never depend on them.
+ * Library extension without a reference counterpart (the reference hard-codes 1024 threads and
+ * 540 batches per launch, include/cc_gpu_sketch_alg.h:14-33). */
+gs_status gs_get_tuning(const gs_graph* g, gs_tuning* out);
+gs_status gs_set_tuning(gs_graph* g, const gs_tuning* t);
+
 /* ---- profiling (per-handle CUDA-event timing on the stream each kernel is launched on) ---- */
 typedef struct gs_profile {
   uint64_t ingest_launches;  /* sketch-update kernel launches */

@@ -295,3 +295,32 @@ def test_full_size_rmat_properties(restatement, torch_cuda):
         for a, b in mine.tolist():
             restatement.sketch_update(one, V, seed, (min(a, b) << 32) | max(a, b))
         assert got[v].tobytes() == one.tobytes(), v
+
+
+def test_results_independent_of_tuning(restatement):
+    """Every autotuner candidate produces the same bytes (XOR is order-independent)."""
+    from gpusketch_b200.autotune import get_tuning, set_tuning
+    V, seed = 5000, 41
+    rng = np.random.default_rng(15)
+    star = np.stack([np.zeros(3000, np.uint32), np.arange(1, 3001, dtype=np.uint32)], 1)
+    pairs = np.concatenate([rng.integers(0, V, size=(60000, 2), dtype=np.uint32), star])
+    want = oracle_bytes(restatement, V, seed, pairs)
+    for chunk, warps, r in [(32, 1, 1), (1024, 4, 2), (4096, 8, 3), (100000, 16, 1), (777, 3, 2)]:
+        with gs.GraphSketch(V, seed) as g:
+            set_tuning(g, chunk, warps, r)
+            assert get_tuning(g) == {"chunk": chunk, "warps_per_block": warps, "reg_depth": r}
+            g.ingest_pairs(pairs)
+            assert sketch_bytes(g) == want, (chunk, warps, r)
+
+
+def test_autotune_keeps_sketches(torch_cuda):
+    from gpusketch_b200.autotune import autotune
+    V = 1 << 12
+    d = torch_cuda.empty((1 << 18, 2), dtype=torch_cuda.int32, device="cuda")
+    gs.rmat_stream(12, 1 << 18, 5, out=d)
+    with gs.GraphSketch(V, 9) as g:
+        g.ingest_pairs(d[:1000])
+        before = sketch_bytes(g)
+        best = autotune(g, d, chunks=(512, 4096), warps=(4, 8), reg_depths=(1, 2))
+        assert sketch_bytes(g) == before
+        assert best["reg_depth"] in (1, 2)
