@@ -35,7 +35,7 @@ def set_tuning(g, chunk: int, warps_per_block: int, reg_depth: int) -> None:
     check(_sig().gs_set_tuning(g._h, C.byref(t)), "gs_set_tuning")
 
 
-def autotune(g, sample_pairs, chunks=(1024, 4096, 16384), warps=(4, 8, 16), reg_depths=(1, 2, 3),
+def autotune(g, sample_pairs, chunks=(256, 512, 1024, 2048, 4096), warps=(4, 8, 16), reg_depths=(1, 2),
              repeats: int = 2, table: list | None = None) -> dict:
     """Times every candidate on `sample_pairs` (a CUDA tensor of records) and applies the fastest.
     The sketches are restored afterwards: each candidate ingests the sample twice (XOR cancels)."""
