@@ -80,6 +80,7 @@ SIGNATURES = {
     "gs_set_tuning": (C.c_int, [_P, _P]),
     "gs_profile_enable": (C.c_int, [_P, C.c_int]),
     "gs_profile_read": (C.c_int, [_P, C.POINTER(GsProfile)]),
+    "gs_ingest_pairs_noalloc": (C.c_int, [C.c_uint32, C.c_uint64, C.c_double, _P, C.c_uint64, _P, _P]),
     "gs_last_error": (C.c_char_p, []),
     "gs_gen_er_stream": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.c_double, C.c_double, _P, C.c_uint64, _U64P]),
     "gs_gen_rmat_stream": (C.c_int, [C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,

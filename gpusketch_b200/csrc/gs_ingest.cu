@@ -737,3 +737,58 @@ gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* 
   GsProfScope ps(g, GS_PROF_INGEST, s, 1);
   return ingest_chunks(g, nv, s);
 }
+
+// ---- ingest over caller-supplied scratch ----
+
+size_t gs_scratch_ingest_smem_bytes(const GsGeom& geom, uint32_t warps) {
+  return ingest_smem_bytes(geom.num_columns <= 32 ? 1 : 2, 1, (int)warps);
+}
+
+namespace {
+
+template <int CG, bool SMALL>
+gs_status launch_ingest_scratch(const GsScratchIngest& x, cudaStream_t s) {
+  IngestArgs A;
+  A.off = x.off; A.choff = x.choff; A.nbr = x.nbr; A.sk = x.sketches; A.colmix = x.colmix;
+  A.status = x.status; A.nv = x.geom.V; A.V = x.geom.V; A.C = x.geom.num_columns;
+  A.bkt = x.geom.bkt_per_col; A.nb = x.geom.num_buckets; A.chunk = x.chunk;
+  const size_t smem = ingest_smem_bytes(CG, 1, (int)x.warps);
+  int nb = 0;
+  GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, 1, SMALL>, (int)x.warps * 32, smem));
+  k_ingest<CG, 1, SMALL><<<x.num_sms * (nb > 0 ? nb : 1), x.warps * 32, smem, s>>>(A);
+  GS_CUDA_TRY(cudaGetLastError());
+  return GS_OK;
+}
+
+}  // namespace
+
+gs_status gs_ingest_pairs_on_scratch(const GsScratchIngest& x, cudaStream_t s) {
+  if (x.n == 0) return GS_OK;
+  const uint32_t nv = x.geom.V;
+  PairTag t;
+  t.V = nv; t.num_levels = 1; t.L = 1; t.fixed_level = -1; t.cs_mix = 0;
+  const uint32_t H = x.part_buckets, lb = x.part_lb;
+  const unsigned tiles = (unsigned)((x.n + kPartEdges - 1) / kPartEdges);
+  const int grid2 = x.num_sms * 4;
+  // everything that must start at zero: error word and totals, bucket totals, vertex counts
+  GS_CUDA_TRY(cudaMemsetAsync(x.status, 0, 16 * sizeof(uint32_t), s));
+  GS_CUDA_TRY(cudaMemsetAsync(x.bkt, 0, (size_t)H * sizeof(uint32_t), s));
+  GS_CUDA_TRY(cudaMemsetAsync(x.cnt, 0, (size_t)(nv + 1) * sizeof(uint32_t), s));
+  const uint2* p = reinterpret_cast<const uint2*>(x.pairs);
+  k_part_count<<<tiles, kPartThreads, H * sizeof(uint32_t), s>>>(p, x.n, t, lb, H, x.bkt, x.status);
+  k_part_scan<<<1, kScanThreads, 0, s>>>(x.bkt, H, x.status);
+  k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, x.n, t, lb, H, x.bkt, x.part,
+                                                                       x.records_cap, x.status);
+  k_vert_count<<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.status);
+  const uint32_t stiles = (nv + kScanTile - 1) / kScanTile;
+  k_scan_tiles<<<stiles, kScanThreads, 0, s>>>(x.cnt, nv, x.chunk, x.off, x.choff, x.tile);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(x.tile, stiles, x.off, x.choff, nv, x.status);
+  k_scan_add<<<stiles, kScanThreads, 0, s>>>(x.off, x.choff, x.cnt, x.tile, nv);
+  k_vert_scatter<<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.nbr,
+                                                                                x.records_cap, x.status);
+  GS_CUDA_TRY(cudaGetLastError());
+  const bool small = x.geom.bkt_per_col < (uint32_t)kSlabDepth;
+  if (x.geom.num_columns <= 32)
+    return small ? launch_ingest_scratch<1, true>(x, s) : launch_ingest_scratch<1, false>(x, s);
+  return small ? launch_ingest_scratch<2, true>(x, s) : launch_ingest_scratch<2, false>(x, s);
+}

@@ -117,3 +117,32 @@ void gs_gen_rmat_host(uint32_t log2_v, double a, double b, double c, double dele
                       uint64_t seed, uint64_t first, uint64_t n, uint32_t* pairs);
 
 GsTuning gs_tune_for(const GsGeom& geom, int num_sms);
+
+// Everything one ingest pass over single-level sketches needs, with every scratch buffer supplied by
+// the caller (the allocation-free entry point, gs_noalloc.cu).
+struct GsScratchIngest {
+  const uint32_t* pairs = nullptr;   // device, n interleaved pairs
+  uint64_t n = 0;
+  GsBucket* sketches = nullptr;      // device, [V][num_buckets]
+  GsGeom geom{};
+  const uint64_t* colmix = nullptr;  // device, num_columns + 1 constants
+  uint32_t* status = nullptr;        // device, 16 words
+  uint32_t* cnt = nullptr;           // device, V + 1
+  uint32_t* off = nullptr;           // device, V + 1
+  uint32_t* choff = nullptr;         // device, V + 1
+  uint32_t* tile = nullptr;          // device, 2 * (ceil(V / 4096) + 1)
+  uint32_t* bkt = nullptr;           // device, 4 * buckets + 2
+  uint2* part = nullptr;             // device, records_cap
+  uint32_t* nbr = nullptr;           // device, records_cap
+  uint64_t records_cap = 0;
+  uint32_t part_lb = 9;
+  uint32_t part_buckets = 0;
+  int num_sms = 148;
+  uint32_t chunk = 1024;
+  uint32_t warps = 4;
+};
+
+// Runs the bucketing passes and the sketch update on the buffers of `x` (no allocation).
+gs_status gs_ingest_pairs_on_scratch(const GsScratchIngest& x, cudaStream_t s);
+// Shared-memory bytes of one sketch-update block, for sizing checks by callers of the above.
+size_t gs_scratch_ingest_smem_bytes(const GsGeom& geom, uint32_t warps);

@@ -218,6 +218,24 @@ gs_status gs_profile_enable(gs_graph* g, int enable);
 /* Waits for queued work and returns the counters accumulated since gs_profile_enable. */
 gs_status gs_profile_read(gs_graph* g, gs_profile* out);
 
+/* ---- allocation-free ingest ----
+ * No counterpart in the reference.  For callers that cannot allocate device memory because another
+ * allocator owns it (a framework's caching allocator, an embedded runtime that forbids allocation
+ * after start-up).  XORs n edge records (device pointer, interleaved uint32 pairs) into the caller's
+ * device sketches of a connected-components graph, laid out [V][num_buckets] gs_bucket as
+ * gs_geometry_for(num_vertices, sketches_factor) sizes them; the result equals gs_ingest_pairs on a
+ * gs_graph with the same seed and factor.  Calls no allocator: all scratch is one static device array
+ * of about 2.3 MB that every GPU loading the library holds until exit, set up on a device by the
+ * first call made there (make that first call before any stream capture).  The array is shared by
+ * all calls and keeps the last call's contents, so calls that overlap on the GPU race.  Rejects
+ * num_vertices outside [2, GS_NOALLOC_MAX_VERTICES] and n > GS_NOALLOC_MAX_EDGES with GS_ERR_BAD_ARG.
+ * Runs on `cuda_stream` (may be NULL) on the current device and returns once the update is applied. */
+#define GS_NOALLOC_MAX_VERTICES 65536u
+#define GS_NOALLOC_MAX_EDGES 65536u
+gs_status gs_ingest_pairs_noalloc(uint32_t num_vertices, uint64_t seed, double sketches_factor,
+                                  const uint32_t* pairs, uint64_t n, gs_bucket* sketches,
+                                  void* cuda_stream);
+
 /* Last error message of the calling thread ("" when none). */
 const char* gs_last_error(void);
 
