@@ -96,8 +96,14 @@ __global__ void k_sample_round0(const GsBucket* __restrict__ sk, uint32_t V, uin
 }
 
 __global__ void k_sizes(const uint32_t* __restrict__ parent, uint32_t V, uint32_t* __restrict__ size) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
-    atomicAdd(&size[parent[v]], 1u);
+  // lanes with the same root add together: in late rounds most vertices share the giant root
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < V; base += stride) {
+    const uint32_t v = base + threadIdx.x;
+    const uint32_t r = v < V ? parent[v] : 0xffffffffu;
+    const uint32_t peers = __match_any_sync(0xffffffffu, r);
+    if (v < V && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&size[r], (uint32_t)__popc(peers));
+  }
 }
 
 // zero the accumulators of non-singleton roots
@@ -111,23 +117,54 @@ __global__ void k_zero_acc(const uint32_t* __restrict__ parent, const uint32_t* 
   }
 }
 
+// Each warp walks kAccRun consecutive vertices; lane l holds buckets l, l+32, l+64 of the column-r slice
+// (bkt_per_col buckets + the deterministic bucket, at most 65) of the current component in registers
+// and flushes them with red.global.xor when the component changes.  Once a giant component has
+// formed, runs are long and its accumulator sees one atomic per bucket per run instead of per vertex.
+constexpr uint32_t kAccRun = 32;
+
+__device__ __forceinline__ void flush_acc(GsBucket* __restrict__ acc, uint32_t root, uint32_t w, const uint64_t* a,
+                                          const uint64_t* g) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const uint32_t j = lane_id() + 32u * k;
+    if (j < w && (a[k] | g[k])) {
+      atomicXor(reinterpret_cast<unsigned long long*>(&acc[(size_t)root * w + j].alpha), (unsigned long long)a[k]);
+      atomicXor(reinterpret_cast<unsigned long long*>(&acc[(size_t)root * w + j].gamma), (unsigned long long)g[k]);
+    }
+  }
+}
+
 __global__ void k_accumulate(const GsBucket* __restrict__ sk, const uint32_t* __restrict__ parent,
                              const uint32_t* __restrict__ size, uint32_t V, uint32_t nb, uint32_t bkt,
                              uint32_t round, GsBucket* __restrict__ acc) {
   const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   const uint32_t w = bkt + 1;
-  for (uint32_t v = w0; v < V; v += nw) {
-    const uint32_t root = parent[v];
-    if (size[root] <= 1) continue;
-    const GsBucket* base = sk + (size_t)v * nb;
-    GsBucket* dst = acc + (size_t)root * w;
-    for (uint32_t j = lane_id(); j < w; j += 32) {
-      const GsBucket b = j < bkt ? base[(size_t)round * bkt + j] : base[nb - 1];
-      if (b.alpha | b.gamma) {
-        atomicXor(reinterpret_cast<unsigned long long*>(&dst[j].alpha), (unsigned long long)b.alpha);
-        atomicXor(reinterpret_cast<unsigned long long*>(&dst[j].gamma), (unsigned long long)b.gamma);
+  for (uint32_t start = w0 * kAccRun; start < V; start += nw * kAccRun) {
+    const uint32_t end = min(V, start + kAccRun);
+    uint32_t cur = 0xffffffffu;
+    uint64_t a[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+    for (uint32_t v = start; v < end; v++) {
+      const uint32_t root = parent[v];
+      if (size[root] <= 1) continue;
+      if (root != cur) {
+        if (cur != 0xffffffffu) flush_acc(acc, cur, w, a, g);
+        cur = root;
+#pragma unroll
+        for (int k = 0; k < 3; k++) a[k] = g[k] = 0;
+      }
+      const GsBucket* base = sk + (size_t)v * nb;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const uint32_t j = lane_id() + 32u * k;
+        if (j < w) {
+          const GsBucket b = j < bkt ? base[(size_t)round * bkt + j] : base[nb - 1];
+          a[k] ^= b.alpha;
+          g[k] ^= b.gamma;
+        }
       }
     }
+    if (cur != 0xffffffffu) flush_acc(acc, cur, w, a, g);
   }
 }
 
@@ -233,8 +270,8 @@ gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStrea
         k_sizes<<<grid_threads(g, V, 256), 256, 0, s>>>(g->d_parent, V, g->d_size);
         k_zero_acc<<<grid_threads(g, (uint64_t)V * (bkt + 1), 256), 256, 0, s>>>(g->d_parent, g->d_size, V,
                                                                                 bkt + 1, g->d_acc);
-        k_accumulate<<<grid_threads(g, (uint64_t)V * 32, 256), 256, 0, s>>>(sk, g->d_parent, g->d_size, V, nb,
-                                                                           bkt, round, g->d_acc);
+        k_accumulate<<<grid_threads(g, (uint64_t)(V + kAccRun - 1) / kAccRun * 32, 256), 256, 0, s>>>(
+            sk, g->d_parent, g->d_size, V, nb, bkt, round, g->d_acc);
         k_sample_roots<<<grid_threads(g, (uint64_t)V * 32, 256), 256, 0, s>>>(
             sk, g->d_acc, g->d_parent, g->d_size, V, nb, bkt, round, csmix, g->d_res, g->d_samp);
       }
