@@ -403,6 +403,32 @@ __device__ __forceinline__ void xor_bucket_global(GsBucket* p, uint64_t a, uint6
   atomicXor(reinterpret_cast<unsigned long long*>(&p->gamma), (unsigned long long)g);
 }
 
+// XOR one record {mix(k'), checksum} = q into bucket depth d of column c: registers for d < R, the
+// lane's shared-memory row for d < kSlabDepth, HBM beyond; d == bkt (or c >= C) touches nothing.
+template <int R, bool SMALL>
+__device__ __forceinline__ void apply_update(uint4 (&acc)[R], uint4* slab_g, GsBucket* skv, uint32_t c, uint32_t C,
+                                             uint32_t bkt, uint32_t d, const uint4& q) {
+  constexpr int kRows = kSlabDepth - R;
+  const bool live = c < C;
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    const bool hit = live && d == (uint32_t)k && (!SMALL || d < bkt);
+    if (hit) { acc[k].x ^= q.x; acc[k].y ^= q.y; acc[k].z ^= q.z; acc[k].w ^= q.w; }
+  }
+  if (live && d >= (uint32_t)R && (!SMALL || d < bkt)) {
+    if (d < (uint32_t)kSlabDepth) {
+      uint4* p = slab_g + (d - R) * kSlabPitch + (c & 31u);
+      uint4 t = *p;
+      t.x ^= q.x; t.y ^= q.y; t.z ^= q.z; t.w ^= q.w;
+      *p = t;
+    } else if (d < bkt) {
+      xor_bucket_global(skv + (size_t)c * bkt + d, gs_key_unmix(((uint64_t)q.y << 32) | q.x),
+                        ((uint64_t)q.w << 32) | q.z);
+    }
+  }
+  (void)kRows;
+}
+
 // Per lane: buckets of depth < kRegDepth of its column(s) in registers, depth [kRegDepth, kSlabDepth)
 // in a lane-private shared-memory row, deeper ones straight into HBM.  Buckets accumulate
 // {mix(k'), checksum} instead of {edge id, checksum}: gs_key_mix is XOR-linear, so XOR-ing mixed
@@ -471,30 +497,26 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
       rec[lane] = make_uint4((uint32_t)E, (uint32_t)(E >> 32), (uint32_t)cs, (uint32_t)(cs >> 32));
       __syncwarp();
       const uint32_t cnt = min(32u, re - b);
-      for (uint32_t j = 0; j < cnt; j++) {
-        const uint4 q = rec[j];
-        const uint64_t Ej = ((uint64_t)q.y << 32) | q.x;
+      // two records per iteration: their hash chains are independent and overlap in the pipeline
+      uint32_t j = 0;
+      for (; j + 1 < cnt; j += 2) {
+        const uint4 q0 = rec[j], q1 = rec[j + 1];
+        const uint64_t E0 = ((uint64_t)q0.y << 32) | q0.x, E1 = ((uint64_t)q1.y << 32) | q1.x;
 #pragma unroll
         for (int g = 0; g < CG; g++) {
-          const uint32_t c = lane + 32u * g;
-          if (c < C) {
-            const uint32_t d = gs_depth_from_mixed(Ej ^ cmix[g], bkt);  // d == bkt: no bucket
+          const uint32_t d0 = gs_depth_from_mixed(E0 ^ cmix[g], bkt);
+          const uint32_t d1 = gs_depth_from_mixed(E1 ^ cmix[g], bkt);
+          apply_update<R, SMALL>(acc[g], slab + g * kRows * kSlabPitch, skv, lane + 32u * g, C, bkt, d0, q0);
+          apply_update<R, SMALL>(acc[g], slab + g * kRows * kSlabPitch, skv, lane + 32u * g, C, bkt, d1, q1);
+        }
+      }
+      if (j < cnt) {
+        const uint4 q0 = rec[j];
+        const uint64_t E0 = ((uint64_t)q0.y << 32) | q0.x;
 #pragma unroll
-            for (int k = 0; k < kRegDepth; k++) {
-              const bool hit = SMALL ? (d == (uint32_t)k && d < bkt) : d == (uint32_t)k;
-              if (hit) { acc[g][k].x ^= q.x; acc[g][k].y ^= q.y; acc[g][k].z ^= q.z; acc[g][k].w ^= q.w; }
-            }
-            if (d >= (uint32_t)kRegDepth && (!SMALL || d < bkt)) {
-              if (d < (uint32_t)kSlabDepth) {
-                uint4* p = slab + (g * kRows + (d - kRegDepth)) * kSlabPitch + lane;
-                uint4 t = *p;
-                t.x ^= q.x; t.y ^= q.y; t.z ^= q.z; t.w ^= q.w;
-                *p = t;
-              } else if (d < bkt) {
-                xor_bucket_global(skv + (size_t)c * bkt + d, gs_key_unmix(Ej), ((uint64_t)q.w << 32) | q.z);
-              }
-            }
-          }
+        for (int g = 0; g < CG; g++) {
+          const uint32_t d0 = gs_depth_from_mixed(E0 ^ cmix[g], bkt);
+          apply_update<R, SMALL>(acc[g], slab + g * kRows * kSlabPitch, skv, lane + 32u * g, C, bkt, d0, q0);
         }
       }
       __syncwarp();
