@@ -11,35 +11,57 @@
 //   the round as modified; the loop stops at the first unmodified round, and a round
 //   r >= num_samples is the reference's OutOfSamplesException (src/sketch.cpp:111-113,173-177).
 //
-// Device mapping:
-//   k_sample_*     one warp per supernode: lane j checks bucket j of the column (and j+32) with one
-//                  XXH3 each (Bucket_Boruvka::is_good, include/bucket.h:65-67); the sample is the
-//                  deterministic bucket when it is zero/good, else the first good bucket by depth,
-//                  found with one ballot (Sketch::sample, src/sketch.cpp:110-132).
-//   k_accumulate   one warp per vertex of a non-singleton component XORs its column-r slice into
-//                  the component accumulator with red.global.xor (the accumulators, 16*(bkt+1) B
-//                  per component, stay resident in L2 at the sizes here).
-//   k_union        CAS hooking of the larger root under the smaller root; the root of every
-//                  component is its minimum vertex id, so labels are deterministic.
-//   k_compress     full path compression, so every parent entry is a root after each round.
-// Every DSU walk is bounded by V+64 steps and reports GS_DEV_ERR_DSU_LIMIT instead of spinning.
+// All rounds run inside one persistent kernel (k_boruvka), so a query is one launch and one
+// read-back instead of a host round trip per round.  Its blocks are co-resident (cooperative
+// launch) and meet at a grid barrier between phases; every barrier wait is bounded and reports
+// GS_DEV_ERR_TIMEOUT instead of spinning forever.  Several independent graphs ("tenants", each with
+// its own geometry and seed) can share one launch: their vertices are disjoint ranges of one vertex
+// space, their rounds advance together, and a tenant whose round was unmodified stops taking part,
+// so each tenant's partition, round count and out-of-samples status equal a query run alone.
+//
+// Per round:
+//   sizes       component sizes from the compressed parent array (warp-aggregated atomics); the
+//               size array also freezes the round's root set, so sampling and unions can share a phase
+//   accumulate  warps walk runs of consecutive vertices and XOR column r + the deterministic bucket
+//               into a register accumulator per component, flushed with red.global.xor when the
+//               component changes (one flush per run once a giant component forms)
+//   sample      one warp per root: lane j checks bucket j (and j+32) with one XXH3 each
+//               (Bucket_Boruvka::is_good, include/bucket.h:65-67); the deterministic bucket is zero /
+//               good first, else the first good bucket by depth, found with one ballot
+//               (Sketch::sample, src/sketch.cpp:110-132); the sampled edge is unioned at once
+//   compress    full path compression
+// DSU: CAS hooking of the larger root under the smaller (include/dsu.h:155-167 unions by random
+// priority instead), so every component's root is its minimum vertex id and labels are deterministic;
+// every walk is bounded by V+64 steps and reports GS_DEV_ERR_DSU_LIMIT.
 #include "gs_internal.h"
 
 namespace {
 
-constexpr uint32_t kGood = 0, kZero = 1, kFail = 2, kSkip = 3;
+constexpr uint32_t kGood = 0, kZero = 1, kFail = 2;
+constexpr uint32_t kAccRun = 32;                 // vertices per accumulation run
+constexpr uint32_t kBarrierSpinLimit = 1u << 24; // x ~64 ns naps: about a second
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
+  return *reinterpret_cast<const volatile uint32_t*>(p);
+}
+
+// loads of data written by other blocks earlier in the same launch bypass L1
+__device__ __forceinline__ GsBucket ld_bucket_cg(const GsBucket* p) {
+  const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(p));
+  return GsBucket{v.x, v.y};
+}
 
 __device__ __forceinline__ bool is_good(const GsBucket& b, uint64_t csmix) {
   return gs_hash_tail(gs_key_mix(b.alpha) ^ csmix) == b.gamma;
 }
 
 // Sketch::sample on one column: all lanes of the warp call it and get the same answer.
-__device__ __forceinline__ void sample_warp(const GsBucket* __restrict__ col, const GsBucket* __restrict__ det,
-                                            uint32_t bkt, uint64_t csmix, uint32_t* code, uint64_t* idx) {
+__device__ __forceinline__ void sample_warp(const GsBucket* col, const GsBucket* det, uint32_t bkt, uint64_t csmix,
+                                            uint32_t* code, uint64_t* idx) {
   const uint32_t lane = lane_id();
-  const GsBucket d = *det;
+  const GsBucket d = ld_bucket_cg(det);
   if (d.alpha == 0 && d.gamma == 0) { *code = kZero; *idx = 0; return; }
   if (is_good(d, csmix)) { *code = kGood; *idx = d.alpha; return; }
   for (uint32_t j0 = 0; j0 < bkt; j0 += 32) {
@@ -47,15 +69,14 @@ __device__ __forceinline__ void sample_warp(const GsBucket* __restrict__ col, co
     bool good = false;
     uint64_t a = 0;
     if (j < bkt) {
-      const GsBucket b = col[j];
+      const GsBucket b = ld_bucket_cg(col + j);
       a = b.alpha;
       good = is_good(b, csmix);
     }
     const uint32_t m = __ballot_sync(0xffffffffu, good);
     if (m) {
-      const uint32_t src = __ffs(m) - 1;
       *code = kGood;
-      *idx = __shfl_sync(0xffffffffu, a, src);
+      *idx = __shfl_sync(0xffffffffu, a, __ffs(m) - 1);
       return;
     }
   }
@@ -63,234 +84,321 @@ __device__ __forceinline__ void sample_warp(const GsBucket* __restrict__ col, co
   *idx = 0;
 }
 
-__device__ __forceinline__ uint32_t ld_parent(const uint32_t* p, uint32_t x) {
-  return *reinterpret_cast<const volatile uint32_t*>(p + x);
-}
-
-__device__ __forceinline__ uint32_t dsu_find(const uint32_t* parent, uint32_t x, uint32_t limit,
-                                             uint32_t* status) {
+__device__ __forceinline__ uint32_t dsu_find(const uint32_t* parent, uint32_t x, uint32_t limit, uint32_t* err) {
   for (uint32_t it = 0; it < limit; it++) {
-    const uint32_t p = ld_parent(parent, x);
+    const uint32_t p = ld_volatile(parent + x);
     if (p == x) return x;
     x = p;
   }
-  atomicOr(status, (uint32_t)GS_DEV_ERR_DSU_LIMIT);
+  atomicOr(err, (uint32_t)GS_DEV_ERR_DSU_LIMIT);
   return x;
 }
 
-__global__ void k_dsu_init(uint32_t* __restrict__ parent, uint32_t V) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) parent[v] = v;
-}
-
-__global__ void k_sample_round0(const GsBucket* __restrict__ sk, uint32_t V, uint32_t nb, uint32_t bkt,
-                                uint32_t col, uint64_t csmix, uint32_t* __restrict__ res,
-                                uint64_t* __restrict__ samp) {
-  const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t v = w0; v < V; v += nw) {
-    const GsBucket* base = sk + (size_t)v * nb;
-    uint32_t code;
-    uint64_t idx;
-    sample_warp(base + (size_t)col * bkt, base + (nb - 1), bkt, csmix, &code, &idx);
-    if (lane_id() == 0) { res[v] = code; samp[v] = idx; }
+// union of global vertices a, b; true when it joined two components
+__device__ __forceinline__ bool dsu_union(uint32_t* parent, uint32_t a, uint32_t b, uint32_t limit, uint32_t* err) {
+  for (uint32_t it = 0; it < limit; it++) {
+    a = dsu_find(parent, a, limit, err);
+    b = dsu_find(parent, b, limit, err);
+    if (a == b) return false;
+    if (a < b) { const uint32_t t = a; a = b; b = t; }
+    if (atomicCAS(&parent[a], a, b) == a) return true;
   }
+  atomicOr(err, (uint32_t)GS_DEV_ERR_DSU_LIMIT);
+  return false;
 }
 
-__global__ void k_sizes(const uint32_t* __restrict__ parent, uint32_t V, uint32_t* __restrict__ size) {
-  // lanes with the same root add together: in late rounds most vertices share the giant root
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < V; base += stride) {
-    const uint32_t v = base + threadIdx.x;
-    const uint32_t r = v < V ? parent[v] : 0xffffffffu;
-    const uint32_t peers = __match_any_sync(0xffffffffu, r);
-    if (v < V && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&size[r], (uint32_t)__popc(peers));
+// Grid-wide barrier of a co-resident launch.  Returns false when any block gave up waiting.
+__device__ bool grid_sync(uint32_t* count, uint32_t* gen, uint32_t* err) {
+  __shared__ uint32_t s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t ok = 1;
+    const uint32_t g = ld_volatile(gen);
+    __threadfence();
+    if (atomicAdd(count, 1u) == gridDim.x - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      uint32_t it = 0;
+      while (ld_volatile(gen) == g) {
+        if (++it > kBarrierSpinLimit || (ld_volatile(err) & GS_DEV_ERR_TIMEOUT)) {
+          atomicOr(err, (uint32_t)GS_DEV_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok && !(ld_volatile(err) & GS_DEV_ERR_TIMEOUT);
   }
+  __syncthreads();
+  return s_ok != 0;
 }
 
-// zero the accumulators of non-singleton roots
-__global__ void k_zero_acc(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ size, uint32_t V,
-                           uint32_t w, GsBucket* __restrict__ acc) {
-  const uint64_t total = (uint64_t)V * w;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t v = (uint32_t)(i / w);
-    if (parent[v] == v && size[v] > 1) acc[i] = GsBucket{0, 0};
-  }
+struct BorArgs {
+  const GsBucket* sk;          // sketch base the tenants' sk_off index into
+  const GsBorTenant* tenants;  // [T] (device), or nullptr: the single tenant t0
+  GsBorTenant t0;
+  const uint32_t* vtenant;     // [V] tenant of each vertex, nullptr when T == 1
+  uint32_t T, V, W;            // W: accumulator row width, max bkt_per_col + 1
+  uint32_t max_rounds;         // max num_samples over the tenants
+  uint32_t* parent;            // [V]
+  uint32_t* size;              // [V]
+  GsBucket* acc;               // [V][W]
+  uint32_t* forest;            // [2 * forest_cap]
+  uint32_t forest_cap;
+  uint32_t* status;            // [0] error bits [4] forest edges [5] active tenants [6,7] barrier
+  uint32_t* tstate;            // [T][4]: done, modified this round, rounds, out of samples
+};
+
+__device__ __forceinline__ const GsBorTenant& tenant_of(const BorArgs& A, uint32_t t) {
+  return A.tenants ? A.tenants[t] : A.t0;
 }
 
-// Each warp walks kAccRun consecutive vertices; lane l holds buckets l, l+32, l+64 of the column-r slice
-// (bkt_per_col buckets + the deterministic bucket, at most 65) of the current component in registers
-// and flushes them with red.global.xor when the component changes.  Once a giant component has
-// formed, runs are long and its accumulator sees one atomic per bucket per run instead of per vertex.
-constexpr uint32_t kAccRun = 32;
-
-__device__ __forceinline__ void flush_acc(GsBucket* __restrict__ acc, uint32_t root, uint32_t w, const uint64_t* a,
-                                          const uint64_t* g) {
+__device__ __forceinline__ void flush_acc(const BorArgs& A, uint32_t cur, uint32_t w, const uint64_t* a,
+                                          const uint64_t* gm) {
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const uint32_t j = lane_id() + 32u * k;
-    if (j < w && (a[k] | g[k])) {
-      atomicXor(reinterpret_cast<unsigned long long*>(&acc[(size_t)root * w + j].alpha), (unsigned long long)a[k]);
-      atomicXor(reinterpret_cast<unsigned long long*>(&acc[(size_t)root * w + j].gamma), (unsigned long long)g[k]);
+    if (j < w && (a[k] | gm[k])) {
+      atomicXor(reinterpret_cast<unsigned long long*>(&A.acc[(size_t)cur * A.W + j].alpha), (unsigned long long)a[k]);
+      atomicXor(reinterpret_cast<unsigned long long*>(&A.acc[(size_t)cur * A.W + j].gamma), (unsigned long long)gm[k]);
     }
   }
 }
 
-__global__ void k_accumulate(const GsBucket* __restrict__ sk, const uint32_t* __restrict__ parent,
-                             const uint32_t* __restrict__ size, uint32_t V, uint32_t nb, uint32_t bkt,
-                             uint32_t round, GsBucket* __restrict__ acc) {
-  const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t w = bkt + 1;
-  for (uint32_t start = w0 * kAccRun; start < V; start += nw * kAccRun) {
-    const uint32_t end = min(V, start + kAccRun);
-    uint32_t cur = 0xffffffffu;
-    uint64_t a[3] = {0, 0, 0}, g[3] = {0, 0, 0};
-    for (uint32_t v = start; v < end; v++) {
-      const uint32_t root = parent[v];
-      if (size[root] <= 1) continue;
-      if (root != cur) {
-        if (cur != 0xffffffffu) flush_acc(acc, cur, w, a, g);
-        cur = root;
-#pragma unroll
-        for (int k = 0; k < 3; k++) a[k] = g[k] = 0;
+__global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
+  uint32_t* err = A.status;
+  uint32_t* bcount = A.status + 6;
+  uint32_t* bgen = A.status + 7;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+  const uint32_t gwarp = gtid >> 5, gwarps = gthreads >> 5;
+  const uint32_t limit = A.V + 64;
+
+  for (uint32_t v = gtid; v < A.V; v += gthreads) A.parent[v] = v;
+  if (!grid_sync(bcount, bgen, err)) return;
+
+  for (uint32_t round = 0; round < A.max_rounds; round++) {
+    if (round > 0) {
+      // ---- sizes of the round's components (frozen root set) ----
+      for (uint32_t v = gtid; v < A.V; v += gthreads) A.size[v] = 0;
+      if (!grid_sync(bcount, bgen, err)) return;
+      for (uint32_t base = blockIdx.x * blockDim.x; base < A.V; base += gthreads) {
+        const uint32_t v = base + threadIdx.x;
+        uint32_t r = 0xffffffffu;
+        if (v < A.V) {
+          const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
+          if (!ld_volatile(&A.tstate[4 * t])) r = __ldcg(&A.parent[v]);
+        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, r);
+        if (r != 0xffffffffu && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&A.size[r], (uint32_t)__popc(peers));
       }
-      const GsBucket* base = sk + (size_t)v * nb;
+      if (!grid_sync(bcount, bgen, err)) return;
+      // ---- zero the accumulators of non-singleton components ----
+      const uint64_t cells = (uint64_t)A.V * A.W;
+      for (uint64_t i = gtid; i < cells; i += gthreads) {
+        const uint32_t v = (uint32_t)(i / A.W);
+        if (__ldcg(&A.size[v]) > 1) A.acc[i] = GsBucket{0, 0};
+      }
+      if (!grid_sync(bcount, bgen, err)) return;
+      // ---- accumulate column r + the deterministic bucket per component ----
+      for (uint32_t start = gwarp * kAccRun; start < A.V; start += gwarps * kAccRun) {
+        const uint32_t end = min(A.V, start + kAccRun);
+        uint32_t cur = 0xffffffffu, w = 0;
+        uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
+        for (uint32_t v = start; v < end; v++) {
+          const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
+          if (ld_volatile(&A.tstate[4 * t])) continue;
+          const uint32_t root = __ldcg(&A.parent[v]);
+          if (__ldcg(&A.size[root]) <= 1) continue;
+          const GsBorTenant& T = tenant_of(A, t);
+          if (root != cur) {
+            if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
+            cur = root;
+            w = T.bkt + 1;
 #pragma unroll
-      for (int k = 0; k < 3; k++) {
-        const uint32_t j = lane_id() + 32u * k;
-        if (j < w) {
-          const GsBucket b = j < bkt ? base[(size_t)round * bkt + j] : base[nb - 1];
-          a[k] ^= b.alpha;
-          g[k] ^= b.gamma;
+            for (int k = 0; k < 3; k++) a[k] = gm[k] = 0;
+          }
+          const GsBucket* base = A.sk + T.sk_off + (size_t)(v - T.vbase) * T.nb;
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            const uint32_t j = lane_id() + 32u * k;
+            if (j < w) {
+              const GsBucket b = j < T.bkt ? base[(size_t)round * T.bkt + j] : base[T.nb - 1];
+              a[k] ^= b.alpha;
+              gm[k] ^= b.gamma;
+            }
+          }
+        }
+        if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
+      }
+      if (!grid_sync(bcount, bgen, err)) return;
+    }
+
+    // ---- sample every root and union its edge ----
+    for (uint32_t v = gwarp; v < A.V; v += gwarps) {
+      const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
+      volatile uint32_t* ts = A.tstate + 4 * t;
+      if (ts[0]) continue;
+      uint32_t sz = 1;
+      if (round > 0) {
+        sz = __ldcg(&A.size[v]);
+        if (sz == 0) continue;  // not a root this round
+      }
+      const GsBorTenant& T = tenant_of(A, t);
+      const uint32_t col = round == 0 ? T.round0_col : round;
+      if (col >= T.ns) {  // OutOfSamplesException
+        if (lane_id() == 0) ts[3] = 1u;
+        continue;
+      }
+      const GsBucket* own = A.sk + T.sk_off + (size_t)(v - T.vbase) * T.nb;
+      uint32_t code;
+      uint64_t idx;
+      if (sz > 1) {
+        const GsBucket* a = A.acc + (size_t)v * A.W;
+        sample_warp(a, a + T.bkt, T.bkt, T.csmix, &code, &idx);
+      } else {
+        sample_warp(own + (size_t)col * T.bkt, own + (T.nb - 1), T.bkt, T.csmix, &code, &idx);
+      }
+      if (lane_id() == 0) {
+        if (code == kFail) {
+          ts[1] = 1u;
+        } else if (code == kGood) {
+          const uint32_t s = (uint32_t)(idx >> 32), d = (uint32_t)idx;
+          if (s < T.V && d < T.V && s != d) {  // anything else is a checksum collision
+            const uint32_t gs = T.vbase + s, gd = T.vbase + d;
+            if (dsu_union(A.parent, gs, gd, limit, err)) {
+              ts[1] = 1u;
+              const uint32_t k = atomicAdd(&A.status[4], 1u);
+              if (k < A.forest_cap) {
+                A.forest[2 * k] = min(gs, gd);
+                A.forest[2 * k + 1] = max(gs, gd);
+              }
+            }
+          }
         }
       }
     }
-    if (cur != 0xffffffffu) flush_acc(acc, cur, w, a, g);
-  }
-}
+    if (!grid_sync(bcount, bgen, err)) return;
 
-__global__ void k_sample_roots(const GsBucket* __restrict__ sk, const GsBucket* __restrict__ acc,
-                               const uint32_t* __restrict__ parent, const uint32_t* __restrict__ size,
-                               uint32_t V, uint32_t nb, uint32_t bkt, uint32_t round, uint64_t csmix,
-                               uint32_t* __restrict__ res, uint64_t* __restrict__ samp) {
-  const uint32_t w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t v = w0; v < V; v += nw) {
-    uint32_t code = kSkip;
-    uint64_t idx = 0;
-    if (parent[v] == v) {
-      if (size[v] > 1) {
-        const GsBucket* a = acc + (size_t)v * (bkt + 1);
-        sample_warp(a, a + bkt, bkt, csmix, &code, &idx);
+    // ---- compress ----
+    for (uint32_t v = gtid; v < A.V; v += gthreads) A.parent[v] = dsu_find(A.parent, v, limit, err);
+    if (!grid_sync(bcount, bgen, err)) return;
+
+    // ---- per tenant: stop at the first unmodified round ----
+    for (uint32_t t = gtid; t < A.T; t += gthreads) {
+      volatile uint32_t* ts = A.tstate + 4 * t;
+      if (ts[0]) continue;
+      if (ts[3]) {                     // ran out of samples
+        ts[0] = 1u;
+        atomicSub(&A.status[5], 1u);
+      } else if (ts[1]) {              // modified: the next round runs
+        ts[1] = 0u;
+        ts[2] = round + 1;
+        if (round + 1 >= tenant_of(A, t).ns) {
+          ts[3] = 1u;
+          ts[0] = 1u;
+          atomicSub(&A.status[5], 1u);
+        }
       } else {
-        const GsBucket* base = sk + (size_t)v * nb;
-        sample_warp(base + (size_t)round * bkt, base + (nb - 1), bkt, csmix, &code, &idx);
+        ts[0] = 1u;
+        atomicSub(&A.status[5], 1u);
       }
     }
-    if (lane_id() == 0) { res[v] = code; samp[v] = idx; }
+    if (!grid_sync(bcount, bgen, err)) return;
+    if (ld_volatile(&A.status[5]) == 0) return;
   }
 }
 
-// status: [0] error bits, [3] modified flag, [4] forest edge count
-__global__ void k_union(const uint32_t* __restrict__ res, const uint64_t* __restrict__ samp, uint32_t V,
-                        uint32_t* parent, uint32_t* __restrict__ forest, uint32_t* __restrict__ status) {
-  const uint32_t limit = V + 64;
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-    const uint32_t code = res[v];
-    if (code == kFail) { status[3] = 1u; continue; }
-    if (code != kGood) continue;
-    const uint64_t e = samp[v];
-    const uint32_t s = (uint32_t)(e >> 32), d = (uint32_t)e;
-    if (s >= V || d >= V || s == d) continue;  // only a checksum collision yields this
-    uint32_t a = s, b = d;
-    bool merged = false;
-    uint32_t it = 0;
-    for (; it < limit; it++) {
-      a = dsu_find(parent, a, limit, status);
-      b = dsu_find(parent, b, limit, status);
-      if (a == b) break;
-      if (a < b) { const uint32_t t = a; a = b; b = t; }
-      if (atomicCAS(&parent[a], a, b) == a) { merged = true; break; }
-    }
-    if (it == limit) atomicOr(&status[0], (uint32_t)GS_DEV_ERR_DSU_LIMIT);
-    if (merged) {
-      status[3] = 1u;
-      const uint32_t k = atomicAdd(&status[4], 1u);
-      if (k + 1 < V + 1) {  // a forest has at most V-1 edges
-        forest[2 * k] = min(s, d);
-        forest[2 * k + 1] = max(s, d);
-      }
-    }
-  }
-}
-
-__global__ void k_compress(uint32_t* parent, uint32_t V, uint32_t* __restrict__ status) {
-  const uint32_t limit = V + 64;
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-    const uint32_t r = dsu_find(parent, v, limit, status);
-    parent[v] = r;
-  }
-}
-
-inline int grid_threads(gs_graph* g, uint64_t items, int threads) {
-  uint64_t want = (items + threads - 1) / threads;
-  uint64_t cap = (uint64_t)g->num_sms * 16;
-  if (want < 1) want = 1;
-  return (int)(want < cap ? want : cap);
-}
+int g_boruvka_blocks[64] = {};
 
 }  // namespace
 
+gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
+  BorArgs A;
+  A.sk = L.sk;
+  A.tenants = L.T > 1 ? L.tenants : nullptr;
+  A.t0 = L.t0;
+  A.vtenant = L.T > 1 ? L.vtenant : nullptr;
+  A.T = L.T;
+  A.V = L.V;
+  A.W = L.W;
+  A.max_rounds = L.max_rounds;
+  A.parent = L.parent;
+  A.size = L.size;
+  A.acc = L.acc;
+  A.forest = L.forest;
+  A.forest_cap = L.forest_cap;
+  A.status = L.status;
+  A.tstate = L.tstate;
+  int dev = 0;
+  GS_CUDA_TRY(cudaGetDevice(&dev));
+  int& blocks = g_boruvka_blocks[dev < 64 ? dev : 63];
+  if (blocks == 0) {
+    int per_sm = 0, sms = 0;
+    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_boruvka, 256, 0));
+    GS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    blocks = (per_sm > 2 ? 2 : (per_sm > 0 ? per_sm : 1)) * sms;
+  }
+  void* args[] = {&A};
+  GS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_boruvka, dim3(blocks), dim3(256), args, 0, s));
+  return GS_OK;
+}
+
 gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s) {
   const uint32_t V = g->V, nb = g->geom.num_buckets, bkt = g->geom.bkt_per_col;
-  const uint32_t ns = g->geom.num_samples;
-  const GsBucket* sk = g->d_sk + (size_t)level * V * nb;
-  const uint64_t csmix = gs_seed_mix(g->seed);
   g->labels_valid = false;
   g->last_forest_edges = 0;
 
+  GsBorLaunch L;
+  L.sk = g->d_sk + (size_t)level * V * nb;
+  L.t0.sk_off = 0;
+  L.t0.vbase = 0;
+  L.t0.V = V;
+  L.t0.nb = nb;
+  L.t0.bkt = bkt;
+  L.t0.ns = g->geom.num_samples;
+  L.t0.round0_col = round0_col;
+  L.t0.csmix = gs_seed_mix(g->seed);
+  L.T = 1;
+  L.V = V;
+  L.W = bkt + 1;
+  L.max_rounds = g->geom.num_samples;
+  L.parent = g->d_parent;
+  L.size = g->d_size;
+  L.acc = g->d_acc;
+  L.forest = g->d_forest;
+  L.forest_cap = V;
+  L.status = g->d_status;
+  L.tstate = g->d_status + 8;
+
+  // status: everything zero except the count of tenants still running
+  g->h_status[15] = 1;
+  GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 16 * sizeof(uint32_t), s));
+  GS_CUDA_TRY(cudaMemcpyAsync(g->d_status + 5, g->h_status + 15, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   {
     GsProfScope ps(g, GS_PROF_QUERY, s, 1);
-    k_dsu_init<<<grid_threads(g, V, 256), 256, 0, s>>>(g->d_parent, V);
+    GS_TRY(gs_boruvka_launch(L, s));
   }
-  GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 8 * sizeof(uint32_t), s));
-  uint32_t round = 0;
-  for (;;) {
-    GS_CUDA_TRY(cudaMemsetAsync(g->d_status + 3, 0, sizeof(uint32_t), s));
-    if (round > 0 && round >= ns) {
-      gs_set_error("sketch ran out of samples after " + std::to_string(round) + " Boruvka rounds");
-      return GS_ERR_SKETCH_FAIL;
-    }
-    if (round == 0 && round0_col >= ns) { gs_set_error("sketch out of samples at round 0"); return GS_ERR_SKETCH_FAIL; }
-    {
-      GsProfScope ps(g, GS_PROF_QUERY, s, round == 0 ? 3 : 6);
-      if (round == 0) {
-        k_sample_round0<<<grid_threads(g, (uint64_t)V * 32, 256), 256, 0, s>>>(sk, V, nb, bkt, round0_col, csmix,
-                                                                               g->d_res, g->d_samp);
-      } else {
-        GS_CUDA_TRY(cudaMemsetAsync(g->d_size, 0, (size_t)V * sizeof(uint32_t), s));
-        k_sizes<<<grid_threads(g, V, 256), 256, 0, s>>>(g->d_parent, V, g->d_size);
-        k_zero_acc<<<grid_threads(g, (uint64_t)V * (bkt + 1), 256), 256, 0, s>>>(g->d_parent, g->d_size, V,
-                                                                                bkt + 1, g->d_acc);
-        k_accumulate<<<grid_threads(g, (uint64_t)(V + kAccRun - 1) / kAccRun * 32, 256), 256, 0, s>>>(
-            sk, g->d_parent, g->d_size, V, nb, bkt, round, g->d_acc);
-        k_sample_roots<<<grid_threads(g, (uint64_t)V * 32, 256), 256, 0, s>>>(
-            sk, g->d_acc, g->d_parent, g->d_size, V, nb, bkt, round, csmix, g->d_res, g->d_samp);
-      }
-      k_union<<<grid_threads(g, V, 256), 256, 0, s>>>(g->d_res, g->d_samp, V, g->d_parent, g->d_forest,
-                                                      g->d_status);
-      k_compress<<<grid_threads(g, V, 256), 256, 0, s>>>(g->d_parent, V, g->d_status);
-      GS_CUDA_TRY(cudaGetLastError());
-    }
-    GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    GS_CUDA_TRY(cudaStreamSynchronize(s));
-    if (g->h_status[0] & GS_DEV_ERR_DSU_LIMIT) {
-      gs_set_error("DSU walk exceeded its bound");
-      return GS_ERR_INTERNAL;
-    }
-    if (!g->h_status[3]) break;
-    round++;
+  GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, 15 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GS_CUDA_TRY(cudaStreamSynchronize(s));
+  const uint32_t* st = g->h_status;
+  if (st[0] & GS_DEV_ERR_TIMEOUT) {
+    gs_set_error("a grid barrier of the Boruvka kernel gave up waiting");
+    return GS_ERR_TIMEOUT;
   }
-  g->last_rounds = round;
-  g->last_forest_edges = g->h_status[4] < V ? g->h_status[4] : (V ? V - 1 : 0);
+  if (st[0] & GS_DEV_ERR_DSU_LIMIT) {
+    gs_set_error("DSU walk exceeded its bound");
+    return GS_ERR_INTERNAL;
+  }
+  if (st[8 + 3]) {
+    gs_set_error("sketch ran out of samples after " + std::to_string(st[8 + 2]) + " Boruvka rounds");
+    return GS_ERR_SKETCH_FAIL;
+  }
+  g->last_rounds = st[8 + 2];
+  g->last_forest_edges = st[4] < V ? st[4] : V - 1;
   g->labels_valid = true;
   g->labels_level = level;
   return GS_OK;

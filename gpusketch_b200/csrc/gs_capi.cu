@@ -61,6 +61,10 @@ gs_status check_status(gs_graph* g, cudaStream_t s) {
       gs_set_error("an edge record named a vertex id >= num_vertices; those records were skipped");
       return GS_ERR_BAD_ARG;
     }
+    if (bits & GS_DEV_ERR_TIMEOUT) {
+      gs_set_error("a bounded device-side wait gave up");
+      return GS_ERR_TIMEOUT;
+    }
     gs_set_error("device consistency check failed (bits " + std::to_string(bits) + ")");
     return GS_ERR_INTERNAL;
   }

@@ -149,4 +149,5 @@ enum : uint32_t {
   GS_DEV_ERR_VERTEX_RANGE = 1u,   // an input vertex id >= V
   GS_DEV_ERR_CAPACITY = 2u,       // more records than the scratch holds
   GS_DEV_ERR_DSU_LIMIT = 4u,      // a DSU walk exceeded its iteration bound
+  GS_DEV_ERR_TIMEOUT = 8u,        // a bounded device-side wait (grid barrier) gave up
 };

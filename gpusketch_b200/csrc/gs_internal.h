@@ -106,6 +106,33 @@ gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* 
 // Device Boruvka on one level; forest edges stay in g->d_forest.
 gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s);
 
+// One independent graph of a Boruvka launch (gs_boruvka.cu).
+struct GsBorTenant {
+  uint64_t sk_off;      // bucket offset of the tenant's vertex-0 sketch from the launch's sketch base
+  uint64_t csmix;       // checksum hash constant mix(B(seed))
+  uint32_t vbase;       // first vertex of the tenant in the launch's vertex space
+  uint32_t V, nb, bkt, ns;
+  uint32_t round0_col;  // column sampled in round 0
+};
+
+struct GsBorLaunch {
+  const GsBucket* sk = nullptr;
+  const GsBorTenant* tenants = nullptr;  // device [T] when T > 1
+  GsBorTenant t0{};                      // the tenant when T == 1
+  const uint32_t* vtenant = nullptr;     // device [V] when T > 1
+  uint32_t T = 1, V = 0, W = 0, max_rounds = 0;
+  uint32_t* parent = nullptr;
+  uint32_t* size = nullptr;
+  GsBucket* acc = nullptr;
+  uint32_t* forest = nullptr;
+  uint32_t forest_cap = 0;
+  uint32_t* status = nullptr;            // 8 words: [0] errors [4] forest edges [5] running tenants [6,7] barrier
+  uint32_t* tstate = nullptr;            // [T][4]: done, modified, rounds, out of samples
+};
+
+// All Boruvka rounds of every tenant in one cooperative launch (queued on s, no host sync).
+gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s);
+
 // Exact global min cut (host), gs_mincut.cpp.
 uint64_t gs_exact_min_cut_host(uint32_t V, const uint32_t* pairs, uint64_t m, uint8_t* side);
 
