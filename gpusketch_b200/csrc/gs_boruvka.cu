@@ -197,10 +197,10 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
       }
       if (!grid_sync(bcount, bgen, err)) return;
       // ---- zero the accumulators of non-singleton components ----
-      const uint64_t cells = (uint64_t)A.V * A.W;
-      for (uint64_t i = gtid; i < cells; i += gthreads) {
-        const uint32_t v = (uint32_t)(i / A.W);
-        if (__ldcg(&A.size[v]) > 1) A.acc[i] = GsBucket{0, 0};
+      for (uint32_t v = gwarp; v < A.V; v += gwarps) {
+        if (__ldcg(&A.size[v]) <= 1) continue;
+        GsBucket* row = A.acc + (size_t)v * A.W;
+        for (uint32_t j = lane_id(); j < A.W; j += 32) row[j] = GsBucket{0, 0};
       }
       if (!grid_sync(bcount, bgen, err)) return;
       // ---- accumulate column r + the deterministic bucket per component ----
@@ -340,7 +340,7 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
     int per_sm = 0, sms = 0;
     GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_boruvka, 256, 0));
     GS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    blocks = (per_sm > 2 ? 2 : (per_sm > 0 ? per_sm : 1)) * sms;
+    blocks = (per_sm > 0 ? per_sm : 1) * sms;  // every block co-resident: the cooperative-launch limit
   }
   void* args[] = {&A};
   GS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_boruvka, dim3(blocks), dim3(256), args, 0, s));
