@@ -39,7 +39,7 @@ namespace {
 
 constexpr uint32_t kGood = 0, kZero = 1, kFail = 2;
 constexpr uint32_t kAccRun = 32;                 // vertices per accumulation run
-constexpr uint32_t kBarrierSpinLimit = 1u << 24; // x ~64 ns naps: about a second
+constexpr uint64_t kBarrierWaitNs = 1000000000ull;  // a barrier wait gives up after about a second
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
@@ -107,7 +107,9 @@ __device__ __forceinline__ bool dsu_union(uint32_t* parent, uint32_t a, uint32_t
   return false;
 }
 
-// Grid-wide barrier of a co-resident launch.  Returns false when any block gave up waiting.
+// Grid-wide barrier of a co-resident launch.  Returns false when any block gave up waiting.  The
+// waiting thread backs off exponentially (32 ns .. 1 us) so that hundreds of pollers do not saturate
+// the L2 slice that holds the generation word.
 __device__ bool grid_sync(uint32_t* count, uint32_t* gen, uint32_t* err) {
   __shared__ uint32_t s_ok;
   __syncthreads();
@@ -120,14 +122,18 @@ __device__ bool grid_sync(uint32_t* count, uint32_t* gen, uint32_t* err) {
       __threadfence();
       atomicAdd(gen, 1u);
     } else {
-      uint32_t it = 0;
+      uint32_t sleep_ns = 32, it = 0;
+      uint64_t waited = 0;
       while (ld_volatile(gen) == g) {
-        if (++it > kBarrierSpinLimit || (ld_volatile(err) & GS_DEV_ERR_TIMEOUT)) {
+        __nanosleep(sleep_ns);
+        waited += sleep_ns;
+        if (sleep_ns < 1024) sleep_ns <<= 1;
+        if ((++it & 63u) == 0 && (ld_volatile(err) & GS_DEV_ERR_TIMEOUT)) { ok = 0; break; }
+        if (waited > kBarrierWaitNs) {
           atomicOr(err, (uint32_t)GS_DEV_ERR_TIMEOUT);
           ok = 0;
           break;
         }
-        __nanosleep(64);
       }
     }
     __threadfence();
@@ -169,7 +175,14 @@ __device__ __forceinline__ void flush_acc(const BorArgs& A, uint32_t cur, uint32
   }
 }
 
+// done flags of the tenants, copied from tstate into shared memory once per round
+__device__ __forceinline__ void snapshot_done(const BorArgs& A, uint32_t* s_done) {
+  for (uint32_t t = threadIdx.x; t < A.T; t += blockDim.x) s_done[t] = ld_volatile(&A.tstate[4 * t]);
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
+  extern __shared__ uint32_t s_done[];  // [T]
   uint32_t* err = A.status;
   uint32_t* bcount = A.status + 6;
   uint32_t* bgen = A.status + 7;
@@ -181,6 +194,7 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
   if (!grid_sync(bcount, bgen, err)) return;
 
   for (uint32_t round = 0; round < A.max_rounds; round++) {
+    snapshot_done(A, s_done);
     if (round > 0) {
       // ---- sizes of the round's components (frozen root set) ----
       for (uint32_t v = gtid; v < A.V; v += gthreads) A.size[v] = 0;
@@ -190,7 +204,7 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
         uint32_t r = 0xffffffffu;
         if (v < A.V) {
           const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
-          if (!ld_volatile(&A.tstate[4 * t])) r = __ldcg(&A.parent[v]);
+          if (!s_done[t]) r = __ldcg(&A.parent[v]);
         }
         const uint32_t peers = __match_any_sync(0xffffffffu, r);
         if (r != 0xffffffffu && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&A.size[r], (uint32_t)__popc(peers));
@@ -210,7 +224,7 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
         for (uint32_t v = start; v < end; v++) {
           const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
-          if (ld_volatile(&A.tstate[4 * t])) continue;
+          if (s_done[t]) continue;
           const uint32_t root = __ldcg(&A.parent[v]);
           if (__ldcg(&A.size[root]) <= 1) continue;
           const GsBorTenant& T = tenant_of(A, t);
@@ -240,8 +254,8 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
     // ---- sample every root and union its edge ----
     for (uint32_t v = gwarp; v < A.V; v += gwarps) {
       const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
+      if (s_done[t]) continue;
       volatile uint32_t* ts = A.tstate + 4 * t;
-      if (ts[0]) continue;
       uint32_t sz = 1;
       if (round > 0) {
         sz = __ldcg(&A.size[v]);
@@ -312,8 +326,6 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
   }
 }
 
-int g_boruvka_blocks[64] = {};
-
 }  // namespace
 
 gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
@@ -335,15 +347,13 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
   A.tstate = L.tstate;
   int dev = 0;
   GS_CUDA_TRY(cudaGetDevice(&dev));
-  int& blocks = g_boruvka_blocks[dev < 64 ? dev : 63];
-  if (blocks == 0) {
-    int per_sm = 0, sms = 0;
-    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_boruvka, 256, 0));
-    GS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    blocks = (per_sm > 0 ? per_sm : 1) * sms;  // every block co-resident: the cooperative-launch limit
-  }
+  const size_t smem = (size_t)L.T * sizeof(uint32_t);
+  int per_sm = 0, sms = 0;
+  GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_boruvka, 256, smem));
+  GS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = (per_sm > 0 ? per_sm : 1) * sms;  // every block co-resident: the cooperative-launch limit
   void* args[] = {&A};
-  GS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_boruvka, dim3(blocks), dim3(256), args, 0, s));
+  GS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_boruvka, dim3(blocks), dim3(256), args, smem, s));
   return GS_OK;
 }
 
