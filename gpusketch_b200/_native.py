@@ -53,6 +53,11 @@ class GsProfile(C.Structure):
                 ("kernel_launches", C.c_uint64), ("records_ingested", C.c_uint64)]
 
 
+class GsEngineConfig(C.Structure):
+    _fields_ = [("sketch_budget_bytes", C.c_uint64), ("max_tenants", C.c_uint32), ("max_vertices", C.c_uint32),
+                ("max_tenant_vertices", C.c_uint32), ("device", C.c_int32), ("max_batch_edges", C.c_uint64)]
+
+
 SIGNATURES = {
     "gs_geometry_for": (C.c_int, [C.c_uint32, C.c_double, C.POINTER(GsGeometry)]),
     "gs_hash64": (C.c_uint64, [C.c_uint64, C.c_uint64]),
@@ -81,6 +86,23 @@ SIGNATURES = {
     "gs_profile_enable": (C.c_int, [_P, C.c_int]),
     "gs_profile_read": (C.c_int, [_P, C.POINTER(GsProfile)]),
     "gs_ingest_pairs_noalloc": (C.c_int, [C.c_uint32, C.c_uint64, C.c_double, _P, C.c_uint64, _P, _P]),
+    "gs_engine_create": (C.c_int, [C.POINTER(GsEngineConfig), C.POINTER(_P)]),
+    "gs_engine_destroy": (C.c_int, [_P]),
+    "gs_engine_tenant_bytes": (C.c_int, [C.c_uint32, C.c_double, _U64P]),
+    "gs_engine_add_tenant": (C.c_int, [_P, C.c_uint32, C.c_uint64, C.c_double, _U32P]),
+    "gs_engine_remove_tenant": (C.c_int, [_P, C.c_uint32]),
+    "gs_engine_memory": (C.c_int, [_P, _U64P, _U64P, _U32P]),
+    "gs_engine_set_stream": (C.c_int, [_P, _P]),
+    "gs_engine_ingest": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_int, _P]),
+    "gs_engine_synchronize": (C.c_int, [_P]),
+    "gs_engine_connected_components": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P]),
+    "gs_engine_tenant_geometry": (C.c_int, [_P, C.c_uint32, C.POINTER(GsGeometry)]),
+    "gs_engine_download_sketches": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P]),
+    "gs_engine_write_binary": (C.c_int, [_P, C.c_uint32, C.c_char_p]),
+    "gs_engine_get_tuning": (C.c_int, [_P, _P]),
+    "gs_engine_set_tuning": (C.c_int, [_P, _P]),
+    "gs_engine_profile_enable": (C.c_int, [_P, C.c_int]),
+    "gs_engine_profile_read": (C.c_int, [_P, C.POINTER(GsProfile)]),
     "gs_last_error": (C.c_char_p, []),
     "gs_gen_er_stream": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.c_double, C.c_double, _P, C.c_uint64, _U64P]),
     "gs_gen_rmat_stream": (C.c_int, [C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,

@@ -28,7 +28,8 @@
 //   sample      one warp per root: lane j checks bucket j (and j+32) with one XXH3 each
 //               (Bucket_Boruvka::is_good, include/bucket.h:65-67); the deterministic bucket is zero /
 //               good first, else the first good bucket by depth, found with one ballot
-//               (Sketch::sample, src/sketch.cpp:110-132); the sampled edge is unioned at once
+//               (Sketch::sample, src/sketch.cpp:110-132)
+//   union       one thread per root unions its sampled edge, so thousands of DSU walks overlap
 //   compress    full path compression
 // DSU: CAS hooking of the larger root under the smaller (include/dsu.h:155-167 unions by random
 // priority instead), so every component's root is its minimum vertex id and labels are deterministic;
@@ -39,6 +40,7 @@ namespace {
 
 constexpr uint32_t kGood = 0, kZero = 1, kFail = 2;
 constexpr uint32_t kAccRun = 32;                 // vertices per accumulation run
+constexpr int kAccUnroll = 4;                    // vertices whose loads are in flight together
 constexpr uint64_t kBarrierWaitNs = 1000000000ull;  // a barrier wait gives up after about a second
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -84,11 +86,17 @@ __device__ __forceinline__ void sample_warp(const GsBucket* col, const GsBucket*
   *idx = 0;
 }
 
-__device__ __forceinline__ uint32_t dsu_find(const uint32_t* parent, uint32_t x, uint32_t limit, uint32_t* err) {
+// Root of x.  Path halving: every visited vertex is re-pointed at its grandparent.  Only roots are
+// ever CAS'd and a non-root stays a non-root, so these plain stores only ever move a pointer up
+// to another ancestor.
+__device__ __forceinline__ uint32_t dsu_find(uint32_t* parent, uint32_t x, uint32_t limit, uint32_t* err) {
+  volatile uint32_t* P = parent;
   for (uint32_t it = 0; it < limit; it++) {
-    const uint32_t p = ld_volatile(parent + x);
+    const uint32_t p = P[x];
     if (p == x) return x;
-    x = p;
+    const uint32_t gp = P[p];
+    if (gp != p) P[x] = gp;
+    x = gp;
   }
   atomicOr(err, (uint32_t)GS_DEV_ERR_DSU_LIMIT);
   return x;
@@ -149,10 +157,12 @@ struct BorArgs {
   GsBorTenant t0;
   const uint32_t* vtenant;     // [V] tenant of each vertex, nullptr when T == 1
   uint32_t T, V, W;            // W: accumulator row width, max bkt_per_col + 1
+  uint32_t vlo;                // the kernel works on vertices [vlo, V)
   uint32_t max_rounds;         // max num_samples over the tenants
   uint32_t* parent;            // [V]
   uint32_t* size;              // [V]
   GsBucket* acc;               // [V][W]
+  uint64_t* samp;              // [V] sampled edge of each root this round (global ids), ~0 = none
   uint32_t* forest;            // [2 * forest_cap]
   uint32_t forest_cap;
   uint32_t* status;            // [0] error bits [4] forest edges [5] active tenants [6,7] barrier
@@ -190,16 +200,16 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
   const uint32_t gwarp = gtid >> 5, gwarps = gthreads >> 5;
   const uint32_t limit = A.V + 64;
 
-  for (uint32_t v = gtid; v < A.V; v += gthreads) A.parent[v] = v;
+  for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.parent[v] = v;
   if (!grid_sync(bcount, bgen, err)) return;
 
   for (uint32_t round = 0; round < A.max_rounds; round++) {
     snapshot_done(A, s_done);
     if (round > 0) {
       // ---- sizes of the round's components (frozen root set) ----
-      for (uint32_t v = gtid; v < A.V; v += gthreads) A.size[v] = 0;
+      for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.size[v] = 0;
       if (!grid_sync(bcount, bgen, err)) return;
-      for (uint32_t base = blockIdx.x * blockDim.x; base < A.V; base += gthreads) {
+      for (uint32_t base = A.vlo + blockIdx.x * blockDim.x; base < A.V; base += gthreads) {
         const uint32_t v = base + threadIdx.x;
         uint32_t r = 0xffffffffu;
         if (v < A.V) {
@@ -211,38 +221,69 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
       }
       if (!grid_sync(bcount, bgen, err)) return;
       // ---- zero the accumulators of non-singleton components ----
-      for (uint32_t v = gwarp; v < A.V; v += gwarps) {
+      for (uint32_t v = A.vlo + gwarp; v < A.V; v += gwarps) {
         if (__ldcg(&A.size[v]) <= 1) continue;
         GsBucket* row = A.acc + (size_t)v * A.W;
         for (uint32_t j = lane_id(); j < A.W; j += 32) row[j] = GsBucket{0, 0};
       }
       if (!grid_sync(bcount, bgen, err)) return;
       // ---- accumulate column r + the deterministic bucket per component ----
-      for (uint32_t start = gwarp * kAccRun; start < A.V; start += gwarps * kAccRun) {
+      // kAccUnroll vertices' loads are issued together, then folded into the run's accumulator in order
+      for (uint32_t start = A.vlo + gwarp * kAccRun; start < A.V; start += gwarps * kAccRun) {
         const uint32_t end = min(A.V, start + kAccRun);
         uint32_t cur = 0xffffffffu, w = 0;
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
-        for (uint32_t v = start; v < end; v++) {
-          const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
-          if (s_done[t]) continue;
-          const uint32_t root = __ldcg(&A.parent[v]);
-          if (__ldcg(&A.size[root]) <= 1) continue;
-          const GsBorTenant& T = tenant_of(A, t);
-          if (root != cur) {
-            if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
-            cur = root;
-            w = T.bkt + 1;
+        for (uint32_t v0 = start; v0 < end; v0 += kAccUnroll) {
+          uint32_t root[kAccUnroll], vt[kAccUnroll];
 #pragma unroll
-            for (int k = 0; k < 3; k++) a[k] = gm[k] = 0;
+          for (int u = 0; u < kAccUnroll; u++) {
+            const uint32_t v = v0 + u;
+            root[u] = 0xffffffffu;
+            vt[u] = 0;
+            if (v < end) {
+              vt[u] = A.vtenant ? A.vtenant[v] : 0u;
+              if (!s_done[vt[u]]) root[u] = __ldcg(&A.parent[v]);
+            }
           }
-          const GsBucket* base = A.sk + T.sk_off + (size_t)(v - T.vbase) * T.nb;
 #pragma unroll
-          for (int k = 0; k < 3; k++) {
-            const uint32_t j = lane_id() + 32u * k;
-            if (j < w) {
-              const GsBucket b = j < T.bkt ? base[(size_t)round * T.bkt + j] : base[T.nb - 1];
-              a[k] ^= b.alpha;
-              gm[k] ^= b.gamma;
+          for (int u = 0; u < kAccUnroll; u++)
+            if (root[u] != 0xffffffffu && __ldcg(&A.size[root[u]]) <= 1) root[u] = 0xffffffffu;
+          uint64_t la[kAccUnroll][3], lg[kAccUnroll][3];
+          uint32_t lw[kAccUnroll];
+#pragma unroll
+          for (int u = 0; u < kAccUnroll; u++) {
+            lw[u] = 0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) la[u][k] = lg[u][k] = 0;
+            if (root[u] == 0xffffffffu) continue;
+            const GsBorTenant& T = tenant_of(A, vt[u]);
+            const uint32_t bkt = T.bkt, nb = T.nb;
+            lw[u] = bkt + 1;
+            const GsBucket* base = A.sk + T.sk_off + (size_t)(v0 + u - T.vbase) * nb;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              const uint32_t j = lane_id() + 32u * k;
+              if (j <= bkt) {
+                const GsBucket b = j < bkt ? base[(size_t)round * bkt + j] : base[nb - 1];
+                la[u][k] = b.alpha;
+                lg[u][k] = b.gamma;
+              }
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kAccUnroll; u++) {
+            if (root[u] == 0xffffffffu) continue;
+            if (root[u] != cur) {
+              if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
+              cur = root[u];
+              w = lw[u];
+#pragma unroll
+              for (int k = 0; k < 3; k++) a[k] = gm[k] = 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              a[k] ^= la[u][k];
+              gm[k] ^= lg[u][k];
             }
           }
         }
@@ -251,11 +292,10 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
       if (!grid_sync(bcount, bgen, err)) return;
     }
 
-    // ---- sample every root and union its edge ----
-    for (uint32_t v = gwarp; v < A.V; v += gwarps) {
+    // ---- sample every root: one warp per root, the result to samp[root] ----
+    for (uint32_t v = A.vlo + gwarp; v < A.V; v += gwarps) {
       const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
       if (s_done[t]) continue;
-      volatile uint32_t* ts = A.tstate + 4 * t;
       uint32_t sz = 1;
       if (round > 0) {
         sz = __ldcg(&A.size[v]);
@@ -264,41 +304,55 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
       const GsBorTenant& T = tenant_of(A, t);
       const uint32_t col = round == 0 ? T.round0_col : round;
       if (col >= T.ns) {  // OutOfSamplesException
-        if (lane_id() == 0) ts[3] = 1u;
+        if (lane_id() == 0) A.tstate[4 * t + 3] = 1u;
         continue;
       }
       const GsBucket* own = A.sk + T.sk_off + (size_t)(v - T.vbase) * T.nb;
       uint32_t code;
       uint64_t idx;
       if (sz > 1) {
-        const GsBucket* a = A.acc + (size_t)v * A.W;
-        sample_warp(a, a + T.bkt, T.bkt, T.csmix, &code, &idx);
+        const GsBucket* acc = A.acc + (size_t)v * A.W;
+        sample_warp(acc, acc + T.bkt, T.bkt, T.csmix, &code, &idx);
       } else {
         sample_warp(own + (size_t)col * T.bkt, own + (T.nb - 1), T.bkt, T.csmix, &code, &idx);
       }
       if (lane_id() == 0) {
+        uint64_t e = ~0ull;
         if (code == kFail) {
-          ts[1] = 1u;
+          A.tstate[4 * t + 1] = 1u;
         } else if (code == kGood) {
           const uint32_t s = (uint32_t)(idx >> 32), d = (uint32_t)idx;
-          if (s < T.V && d < T.V && s != d) {  // anything else is a checksum collision
-            const uint32_t gs = T.vbase + s, gd = T.vbase + d;
-            if (dsu_union(A.parent, gs, gd, limit, err)) {
-              ts[1] = 1u;
-              const uint32_t k = atomicAdd(&A.status[4], 1u);
-              if (k < A.forest_cap) {
-                A.forest[2 * k] = min(gs, gd);
-                A.forest[2 * k + 1] = max(gs, gd);
-              }
-            }
-          }
+          if (s < T.V && d < T.V && s != d)  // anything else is a checksum collision
+            e = ((uint64_t)(T.vbase + s) << 32) | (T.vbase + d);
+        }
+        A.samp[v] = e;
+      }
+    }
+    if (!grid_sync(bcount, bgen, err)) return;
+
+    // ---- union the sampled edges: one thread per root, so many DSU walks are in flight ----
+    for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) {
+      const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
+      if (s_done[t]) continue;
+      if (round > 0 && __ldcg(&A.size[v]) == 0) continue;
+      const GsBorTenant& T = tenant_of(A, t);
+      if ((round == 0 ? T.round0_col : round) >= T.ns) continue;
+      const uint64_t e = __ldcg(&A.samp[v]);
+      if (e == ~0ull) continue;
+      const uint32_t gs = (uint32_t)(e >> 32), gd = (uint32_t)e;
+      if (dsu_union(A.parent, gs, gd, limit, err)) {
+        A.tstate[4 * t + 1] = 1u;
+        const uint32_t k = atomicAdd(&A.status[4], 1u);
+        if (k < A.forest_cap) {
+          A.forest[2 * k] = min(gs, gd);
+          A.forest[2 * k + 1] = max(gs, gd);
         }
       }
     }
     if (!grid_sync(bcount, bgen, err)) return;
 
     // ---- compress ----
-    for (uint32_t v = gtid; v < A.V; v += gthreads) A.parent[v] = dsu_find(A.parent, v, limit, err);
+    for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.parent[v] = dsu_find(A.parent, v, limit, err);
     if (!grid_sync(bcount, bgen, err)) return;
 
     // ---- per tenant: stop at the first unmodified round ----
@@ -337,10 +391,12 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
   A.T = L.T;
   A.V = L.V;
   A.W = L.W;
+  A.vlo = L.vlo;
   A.max_rounds = L.max_rounds;
   A.parent = L.parent;
   A.size = L.size;
   A.acc = L.acc;
+  A.samp = L.samp;
   A.forest = L.forest;
   A.forest_cap = L.forest_cap;
   A.status = L.status;
@@ -379,6 +435,7 @@ gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStrea
   L.parent = g->d_parent;
   L.size = g->d_size;
   L.acc = g->d_acc;
+  L.samp = g->d_samp;
   L.forest = g->d_forest;
   L.forest_cap = V;
   L.status = g->d_status;

@@ -9,19 +9,7 @@
 
 namespace {
 
-// Makes the handle's device current for the duration of a call and restores the caller's.
-struct DeviceGuard {
-  int prev = -1;
-  bool ok = true;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess) { ok = false; return; }
-    if (dev >= 0 && dev != prev) ok = cudaSetDevice(dev) == cudaSuccess;
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-  }
-};
+using DeviceGuard = GsDeviceGuard;
 
 #define GS_GUARD(g)                                                       \
   DeviceGuard _guard((g)->device);                                        \
@@ -29,7 +17,9 @@ struct DeviceGuard {
 
 cudaStream_t pick_stream(gs_graph* g, void* s) { return s ? static_cast<cudaStream_t>(s) : g->stream; }
 
-void free_graph(gs_graph* g) {
+}  // namespace
+
+void gs_free_graph(gs_graph* g) {
   if (!g) return;
   cudaFree(g->d_sk); cudaFree(g->d_colmix);
   cudaFree(g->d_cnt); cudaFree(g->d_off); cudaFree(g->d_choff); cudaFree(g->d_tile);
@@ -48,6 +38,8 @@ void free_graph(gs_graph* g) {
   if (g->own_stream) cudaStreamDestroy(g->own_stream);
   delete g;
 }
+
+namespace {
 
 // Checks and clears the device error word after the queued work finished.
 gs_status check_status(gs_graph* g, cudaStream_t s) {
@@ -118,7 +110,7 @@ gs_status gs_graph_create(const gs_graph_config* cfg, gs_graph** out) {
   DeviceGuard guard(dev);
   if (!guard.ok) { gs_set_error("cannot select CUDA device"); return GS_ERR_NO_DEVICE; }
 
-  std::unique_ptr<gs_graph, void (*)(gs_graph*)> g(new gs_graph(), free_graph);
+  std::unique_ptr<gs_graph, void (*)(gs_graph*)> g(new gs_graph(), gs_free_graph);
   g->V = cfg->num_vertices;
   g->num_levels = cfg->num_levels;
   g->num_subgraphs = cfg->num_subgraphs ? cfg->num_subgraphs : cfg->num_levels;
@@ -165,7 +157,7 @@ gs_status gs_graph_destroy(gs_graph* g) {
   if (!g) return GS_OK;
   DeviceGuard guard(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
-  free_graph(g);
+  gs_free_graph(g);
   return GS_OK;
 }
 

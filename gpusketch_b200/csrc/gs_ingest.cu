@@ -31,7 +31,6 @@ namespace {
 constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
 constexpr int kScanTile = kScanThreads * kScanPer;
-constexpr int kMaxRegDepth = 3;    // depths [0, R) of a lane's column live in registers (R <= 3)
 constexpr int kSlabDepth = 10;     // depths [R, 10) in a lane-private shared-memory row
 constexpr int kSlabPitch = 33;     // 32 lanes + 1 pad: rows land on distinct bank groups
 
@@ -393,9 +392,11 @@ struct IngestArgs {
   const uint32_t* choff;
   const uint32_t* nbr;
   GsBucket* sk;
-  const uint64_t* colmix;   // [C] column constants, [C] = checksum constant
+  const uint64_t* colmix;   // [C] column constants, [C] = checksum constant; per tenant: [T][kColStride]
   const uint32_t* status;   // [2] = work chunks
   uint32_t nv, V, C, bkt, nb, chunk;
+  const uint32_t* vtenant;       // tenant of every vertex (tenant variant only)
+  const GsIngTenant* tenants;    // geometry and arena offset of every tenant (tenant variant only)
 };
 
 __device__ __forceinline__ void xor_bucket_global(GsBucket* p, uint64_t a, uint64_t g) {
@@ -436,7 +437,9 @@ __device__ __forceinline__ void apply_update(uint4 (&acc)[R], uint4* slab_g, GsB
 // every record is a single 16-byte broadcast {mix(k'), checksum}.
 // R: depths held in registers.  SMALL: the geometry has bkt_per_col < kSlabDepth (V <= 23), so every
 // path checks the depth against bkt_per_col; otherwise only the rare global path does.
-template <int CG, int R, bool SMALL>
+// TEN: the vertices belong to independent graphs of an engine; each work chunk looks up its tenant's
+// geometry, column constants and arena offset.
+template <int CG, int R, bool SMALL, bool TEN>
 __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
   extern __shared__ uint4 smem[];
   constexpr int kRegDepth = R;
@@ -446,13 +449,18 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
   uint4* slab = smem + (size_t)wib * (kSlabWords + 32);
   uint4* rec = slab + kSlabWords;                     // 32 x {mix(k'), checksum}
 
-  const uint32_t C = A.C, bkt = A.bkt, nb = A.nb, V = A.V;
-  const uint64_t csmix = A.colmix[C];
+  uint32_t C = A.C, bkt = A.bkt, nb = A.nb;
+  const uint32_t V = A.V;
+  uint64_t csmix = 0;
   uint64_t cmix[CG];
+  uint32_t cur_t = 0xffffffffu;
+  if (!TEN) {
+    csmix = A.colmix[C];
 #pragma unroll
-  for (int g = 0; g < CG; g++) {
-    const uint32_t c = lane + 32u * g;
-    cmix[g] = c < C ? A.colmix[c] : 0ull;
+    for (int g = 0; g < CG; g++) {
+      const uint32_t c = lane + 32u * g;
+      cmix[g] = c < C ? A.colmix[c] : 0ull;
+    }
   }
 
   const uint32_t total = A.status[2];
@@ -475,8 +483,31 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
     const bool exclusive = (A.choff[vv + 1] - c0) == 1;
     const uint32_t rb = A.off[vv] + (ch - c0) * A.chunk;
     const uint32_t re = min(A.off[vv + 1], rb + A.chunk);
-    const uint32_t v = vv % V;
-    GsBucket* skv = A.sk + (size_t)vv * nb;
+    uint32_t v, vb = 0;  // vb: first engine vertex id of the tenant (neighbours are stored engine-wide)
+    GsBucket* skv;
+    if (TEN) {
+      const uint32_t t = A.vtenant[vv];
+      const GsIngTenant T = A.tenants[t];
+      if (t != cur_t) {
+        cur_t = t;
+        C = T.C;
+        bkt = T.bkt;
+        nb = T.nb;
+        const uint64_t* cm = A.colmix + (size_t)t * kColStride;
+        csmix = cm[C];
+#pragma unroll
+        for (int g = 0; g < CG; g++) {
+          const uint32_t c = lane + 32u * g;
+          cmix[g] = c < C ? cm[c] : 0ull;
+        }
+      }
+      vb = T.vbase;
+      v = vv - vb;
+      skv = A.sk + T.sk_off + (size_t)v * nb;
+    } else {
+      v = vv % V;
+      skv = A.sk + (size_t)vv * nb;
+    }
 
     for (int i = lane; i < kSlabWords; i += 32) slab[i] = make_uint4(0, 0, 0, 0);
     uint4 acc[CG][kRegDepth];
@@ -490,7 +521,7 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
     for (uint32_t b = rb; b < re; b += 32) {
       const uint32_t r = b + lane;
       const bool valid = r < re;
-      const uint32_t u = valid ? A.nbr[r] : v;
+      const uint32_t u = valid ? A.nbr[r] - vb : v;
       const uint64_t E = gs_key_mix(gs_concat(v, u));
       const uint64_t cs = gs_hash_tail(E ^ csmix);
       if (valid) { det_m ^= E; det_g ^= cs; }
@@ -573,7 +604,7 @@ size_t ingest_smem_bytes(int cg, int r, int warps) {
   return (size_t)warps * (size_t)(cg * (kSlabDepth - r) * kSlabPitch + 32) * sizeof(uint4);
 }
 
-template <int CG, int R, bool SMALL>
+template <int CG, int R, bool SMALL, bool TEN>
 gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   IngestArgs A;
   A.off = g->d_off; A.choff = g->d_choff; A.nbr = g->d_nbr; A.sk = g->d_sk; A.colmix = g->d_colmix;
@@ -584,28 +615,35 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   // the opt-in shared-memory limit is a per-device function attribute; the persistent grid fills
   // every SM with as many blocks as registers and shared memory allow
   struct Cache { size_t smem = 0; int warps = 0; int blocks = 0; };
-  static Cache cache[64];
+  static Cache cache[64];  // per device, per kernel instantiation
   Cache& cc = cache[g->device < 64 ? g->device : 63];
   if (cc.smem != smem || cc.warps != warps) {
-    GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest<CG, R, SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest<CG, R, SMALL, TEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int nb = 0;
-    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, R, SMALL>, warps * 32, smem));
+    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, R, SMALL, TEN>, warps * 32, smem));
     cc.smem = smem;
     cc.warps = warps;
     cc.blocks = nb > 0 ? nb : 1;
   }
-  k_ingest<CG, R, SMALL><<<g->num_sms * cc.blocks, warps * 32, smem, s>>>(A);
+  A.vtenant = TEN ? g->d_vtenant : nullptr;
+  A.tenants = TEN ? g->d_ten : nullptr;
+  k_ingest<CG, R, SMALL, TEN><<<g->num_sms * cc.blocks, warps * 32, smem, s>>>(A);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
 }
 
-template <int CG, bool SMALL>
+template <int CG, bool SMALL, bool TEN>
 gs_status launch_ingest_r(gs_graph* g, uint32_t nv, cudaStream_t s) {
   switch (g->tune.reg_depth) {
-    case 1: return launch_ingest<CG, 1, SMALL>(g, nv, s);
-    case 3: return launch_ingest<CG, 3, SMALL>(g, nv, s);
-    default: return launch_ingest<CG, 2, SMALL>(g, nv, s);
+    case 1: return launch_ingest<CG, 1, SMALL, TEN>(g, nv, s);
+    case 3: return launch_ingest<CG, 3, SMALL, TEN>(g, nv, s);
+    default: return launch_ingest<CG, 2, SMALL, TEN>(g, nv, s);
   }
+}
+
+template <int CG, bool TEN>
+gs_status launch_ingest_s(gs_graph* g, uint32_t nv, bool small, cudaStream_t s) {
+  return small ? launch_ingest_r<CG, true, TEN>(g, nv, s) : launch_ingest_r<CG, false, TEN>(g, nv, s);
 }
 
 }  // namespace
@@ -662,11 +700,11 @@ static gs_status scan_counts(gs_graph* g, uint32_t nv, cudaStream_t s) {
 }
 
 static gs_status ingest_chunks(gs_graph* g, uint32_t nv, cudaStream_t s) {
-  const bool small = g->geom.bkt_per_col < (uint32_t)kSlabDepth;
-  if (g->geom.num_columns <= 32)
-    return small ? launch_ingest_r<1, true>(g, nv, s) : launch_ingest_r<1, false>(g, nv, s);
-  if (g->geom.num_columns <= 64)
-    return small ? launch_ingest_r<2, true>(g, nv, s) : launch_ingest_r<2, false>(g, nv, s);
+  const bool ten = g->d_ten != nullptr;
+  const uint32_t cols = ten ? g->ten_max_cols : g->geom.num_columns;
+  const bool small = (ten ? g->ten_min_bkt : g->geom.bkt_per_col) < (uint32_t)kSlabDepth;
+  if (cols <= 32) return ten ? launch_ingest_s<1, true>(g, nv, small, s) : launch_ingest_s<1, false>(g, nv, small, s);
+  if (cols <= 64) return ten ? launch_ingest_s<2, true>(g, nv, small, s) : launch_ingest_s<2, false>(g, nv, small, s);
   gs_set_error("more than 64 sketch columns are not supported");
   return GS_ERR_BAD_ARG;
 }
@@ -774,10 +812,12 @@ gs_status launch_ingest_scratch(const GsScratchIngest& x, cudaStream_t s) {
   A.off = x.off; A.choff = x.choff; A.nbr = x.nbr; A.sk = x.sketches; A.colmix = x.colmix;
   A.status = x.status; A.nv = x.geom.V; A.V = x.geom.V; A.C = x.geom.num_columns;
   A.bkt = x.geom.bkt_per_col; A.nb = x.geom.num_buckets; A.chunk = x.chunk;
+  A.vtenant = nullptr;
+  A.tenants = nullptr;
   const size_t smem = ingest_smem_bytes(CG, 1, (int)x.warps);
   int nb = 0;
-  GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, 1, SMALL>, (int)x.warps * 32, smem));
-  k_ingest<CG, 1, SMALL><<<x.num_sms * (nb > 0 ? nb : 1), x.warps * 32, smem, s>>>(A);
+  GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, 1, SMALL, false>, (int)x.warps * 32, smem));
+  k_ingest<CG, 1, SMALL, false><<<x.num_sms * (nb > 0 ? nb : 1), x.warps * 32, smem, s>>>(A);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
 }

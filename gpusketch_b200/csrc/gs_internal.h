@@ -6,6 +6,16 @@
 
 #include "gs_common.cuh"
 
+// Column-constant row of one engine tenant: num_columns column constants, then the checksum constant.
+constexpr uint32_t kColStride = 65;
+
+// Geometry and arena placement of one engine tenant, as the ingest kernels read it.
+struct GsIngTenant {
+  uint64_t sk_off;   // bucket offset of the tenant's vertex-0 sketch in the arena
+  uint32_t vbase;    // first vertex of the tenant in the engine's vertex space
+  uint32_t V, C, bkt, nb, pad;
+};
+
 // Ingest tuning knobs (picked per geometry by gs_tune_for; overridable through
 // gs_set_tuning for the autotuner).
 struct GsTuning {
@@ -34,6 +44,12 @@ struct gs_graph {
   // ---- resident state ----
   GsBucket* d_sk = nullptr;    // [num_levels][V][num_buckets]
   uint64_t* d_colmix = nullptr;  // [num_columns] mix(B(seed+5c)), then [num_columns] = mix(B(seed))
+
+  // ---- engine tenants (set only on the plumbing handle of a gs_engine) ----
+  const uint32_t* d_vtenant = nullptr;  // [V] tenant of each vertex of the engine's vertex space
+  const GsIngTenant* d_ten = nullptr;   // tenant geometry table; d_colmix then holds kColStride per tenant
+  uint32_t ten_max_cols = 0;            // most columns of any live tenant
+  uint32_t ten_min_bkt = 0;             // fewest buckets per column of any live tenant
 
   // ---- ingest scratch ----
   uint64_t nv_cap = 0;         // virtual vertices the per-vertex arrays hold (num_levels*V)
@@ -79,6 +95,23 @@ struct gs_graph {
   uint64_t records_total = 0;
 };
 
+// Makes a device current for the duration of a call and restores the caller's.
+struct GsDeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit GsDeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) { ok = false; return; }
+    if (dev >= 0 && dev != prev) ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~GsDeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Frees every buffer a handle owns, then the handle.
+void gs_free_graph(gs_graph* g);
+
 enum GsProfClass { GS_PROF_INGEST = 0, GS_PROF_BUCKET = 1, GS_PROF_QUERY = 2 };
 
 // Brackets a group of `launches` kernel launches of one class with CUDA events on stream s.
@@ -121,9 +154,11 @@ struct GsBorLaunch {
   GsBorTenant t0{};                      // the tenant when T == 1
   const uint32_t* vtenant = nullptr;     // device [V] when T > 1
   uint32_t T = 1, V = 0, W = 0, max_rounds = 0;
+  uint32_t vlo = 0;                      // vertices [vlo, V) take part
   uint32_t* parent = nullptr;
   uint32_t* size = nullptr;
   GsBucket* acc = nullptr;
+  uint64_t* samp = nullptr;              // [V]
   uint32_t* forest = nullptr;
   uint32_t forest_cap = 0;
   uint32_t* status = nullptr;            // 8 words: [0] errors [4] forest edges [5] running tenants [6,7] barrier

@@ -236,6 +236,71 @@ gs_status gs_ingest_pairs_noalloc(uint32_t num_vertices, uint64_t seed, double s
                                   const uint32_t* pairs, uint64_t n, gs_bucket* sketches,
                                   void* cuda_stream);
 
+/* ---- multi-tenant engine: many independent connected-components graphs on one GPU ----
+ *
+ * No single reference counterpart: the reference runs one CCSketchAlg per process.  Each tenant is
+ * a graph with its own vertex count, seed and sketches_factor whose sketches are bit-identical to
+ * a gs_graph (equivalently a reference CCSketchAlg) with the same parameters fed the same records;
+ * tenants never share a bucket, so a tenant's sketches and answers do not depend on the others.
+ *
+ *   tenant sketches  [V][num_buckets] gs_bucket inside the engine's device arena (first fit).
+ *   vertex space     each tenant owns V consecutive ids of the engine's vertex space.
+ *   slice            a run of records of one tenant inside one ingest call.
+ *
+ * Admission: gs_engine_add_tenant fails with GS_ERR_OOM when the arena, the vertex space or the
+ * tenant slots cannot hold the tenant; removing tenants frees their space.  An engine handle is
+ * not thread-safe. */
+typedef struct gs_engine gs_engine;
+
+typedef struct gs_engine_config {
+  uint64_t sketch_budget_bytes;  /* device arena for tenant sketches (the admission limit) */
+  uint32_t max_tenants;          /* tenant slots (1..65535) */
+  uint32_t max_vertices;         /* engine vertex space: total V over live tenants */
+  uint32_t max_tenant_vertices;  /* largest V of one tenant (sizes the Boruvka scratch) */
+  int32_t device;                /* CUDA device ordinal; < 0 = current device */
+  uint64_t max_batch_edges;      /* records per internal ingest pass (0 = 2^25) */
+} gs_engine_config;
+
+gs_status gs_engine_create(const gs_engine_config* cfg, gs_engine** out);
+gs_status gs_engine_destroy(gs_engine* e);
+/* Device bytes the sketches of one tenant take (what admission charges). */
+gs_status gs_engine_tenant_bytes(uint32_t num_vertices, double sketches_factor, uint64_t* bytes);
+/* Admits a tenant with zeroed sketches (CCSketchAlg(num_vertices, seed, config) with
+ * config.sketches_factor; src/cc_sketch_alg.cpp:11-55).  GS_ERR_OOM: not admitted now. */
+gs_status gs_engine_add_tenant(gs_engine* e, uint32_t num_vertices, uint64_t seed, double sketches_factor,
+                               uint32_t* tenant);
+gs_status gs_engine_remove_tenant(gs_engine* e, uint32_t tenant);
+/* Sketch bytes in use by live tenants, the arena size, and the live tenant count. */
+gs_status gs_engine_memory(const gs_engine* e, uint64_t* used, uint64_t* capacity, uint32_t* live_tenants);
+gs_status gs_engine_set_stream(gs_engine* e, void* cuda_stream);
+/* Ingests num_slices slices in one pass: slice i is records [slice_offsets[i], slice_offsets[i+1])
+ * of `pairs` (interleaved tenant-local uint32 vertex ids) for tenant slice_tenants[i].  Per tenant
+ * this is gs_ingest_pairs; the bucketing and the sketch update of all slices run as one launch
+ * each.  pairs is a device pointer when pairs_on_device != 0; the slice tables are host arrays.  A
+ * record naming a vertex >= its tenant's V is skipped and reported as GS_ERR_BAD_ARG by the next
+ * gs_engine_synchronize or query. */
+gs_status gs_engine_ingest(gs_engine* e, const uint32_t* slice_tenants, const uint64_t* slice_offsets,
+                           uint32_t num_slices, const uint32_t* pairs, int pairs_on_device, void* cuda_stream);
+gs_status gs_engine_synchronize(gs_engine* e);
+/* connected_components() of `count` distinct tenants in one device Boruvka launch.  labels
+ * (host, may be NULL) receives each listed tenant's V labels back to back in list order, each the
+ * smallest tenant-local vertex id of its component; num_cc[i] and rounds[i] (may be NULL) are the
+ * component count and Boruvka rounds of tenants[i].  GS_ERR_SKETCH_FAIL when a listed tenant ran
+ * out of samples (OutOfSamplesException); the others' results are still written. */
+gs_status gs_engine_connected_components(gs_engine* e, const uint32_t* tenants, uint32_t count, uint32_t* labels,
+                                         uint32_t* num_cc, uint32_t* rounds);
+gs_status gs_engine_tenant_geometry(const gs_engine* e, uint32_t tenant, gs_geometry* out);
+/* Tenant sketches of vertices [first, first+count) to host memory, in the write_binary layout. */
+gs_status gs_engine_download_sketches(gs_engine* e, uint32_t tenant, uint32_t first, uint32_t count,
+                                      gs_bucket* out);
+/* Per-tenant checkpoint in the reference's write_binary format (src/cc_sketch_alg.cpp:57-91);
+ * gs_read_binary reloads it as a gs_graph. */
+gs_status gs_engine_write_binary(gs_engine* e, uint32_t tenant, const char* path);
+gs_status gs_engine_get_tuning(const gs_engine* e, gs_tuning* out);
+gs_status gs_engine_set_tuning(gs_engine* e, const gs_tuning* t);
+gs_status gs_engine_profile_enable(gs_engine* e, int enable);
+gs_status gs_engine_profile_read(gs_engine* e, gs_profile* out);
+
 /* Last error message of the calling thread ("" when none). */
 const char* gs_last_error(void);
 
