@@ -19,18 +19,19 @@
 // space, their rounds advance together, and a tenant whose round was unmodified stops taking part,
 // so each tenant's partition, round count and out-of-samples status equal a query run alone.
 //
-// Per round:
+// Per round (five grid barriers):
 //   sizes       component sizes from the compressed parent array (warp-aggregated atomics); the
-//               size array also freezes the round's root set, so sampling and unions can share a phase
+//               size array also freezes the round's root set for sampling and unions
 //   accumulate  warps walk runs of consecutive vertices and XOR column r + the deterministic bucket
 //               into a register accumulator per component, flushed with red.global.xor when the
 //               component changes (one flush per run once a giant component forms)
-//   sample      one warp per root: lane j checks bucket j (and j+32) with one XXH3 each
-//               (Bucket_Boruvka::is_good, include/bucket.h:65-67); the deterministic bucket is zero /
-//               good first, else the first good bucket by depth, found with one ballot
-//               (Sketch::sample, src/sketch.cpp:110-132)
+//   sample      a warp finds 32 roots at a time with one ballot, then samples each: lane j checks
+//               bucket j (and j+32) with one XXH3 each (Bucket_Boruvka::is_good, include/bucket.h:
+//               65-67); the deterministic bucket is zero / good first, else the first good bucket by
+//               depth (Sketch::sample, src/sketch.cpp:110-132); the component's accumulator row is
+//               zeroed once read, so rows are all zero between rounds and between launches
 //   union       one thread per root unions its sampled edge, so thousands of DSU walks overlap
-//   compress    full path compression
+//   compress    full path compression, sizes cleared, per-tenant stop / out-of-samples decisions
 // DSU: CAS hooking of the larger root under the smaller (include/dsu.h:155-167 unions by random
 // priority instead), so every component's root is its minimum vertex id and labels are deterministic;
 // every walk is bounded by V+64 steps and reports GS_DEV_ERR_DSU_LIMIT.
@@ -39,8 +40,9 @@
 namespace {
 
 constexpr uint32_t kGood = 0, kZero = 1, kFail = 2;
-constexpr uint32_t kAccRun = 32;                 // vertices per accumulation run
-constexpr int kAccUnroll = 4;                    // vertices whose loads are in flight together
+constexpr uint32_t kAccRun = 16;                 // vertices a warp stages in shared memory at once
+constexpr uint32_t kThreads = 256;
+constexpr uint32_t kWarps = kThreads / 32;
 constexpr uint64_t kBarrierWaitNs = 1000000000ull;  // a barrier wait gives up after about a second
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -55,30 +57,36 @@ __device__ __forceinline__ GsBucket ld_bucket_cg(const GsBucket* p) {
   return GsBucket{v.x, v.y};
 }
 
+// 16-byte global -> shared copy that completes asynchronously (waited for with cp_async_wait_all)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __device__ __forceinline__ bool is_good(const GsBucket& b, uint64_t csmix) {
   return gs_hash_tail(gs_key_mix(b.alpha) ^ csmix) == b.gamma;
 }
 
-// Sketch::sample on one column: all lanes of the warp call it and get the same answer.
+// Sketch::sample on one column: all lanes of the warp call it and get the same answer.  The
+// deterministic bucket and the first 32 column buckets are loaded together.
 __device__ __forceinline__ void sample_warp(const GsBucket* col, const GsBucket* det, uint32_t bkt, uint64_t csmix,
                                             uint32_t* code, uint64_t* idx) {
   const uint32_t lane = lane_id();
   const GsBucket d = ld_bucket_cg(det);
+  GsBucket b = GsBucket{0, 0};
+  if (lane < bkt) b = ld_bucket_cg(col + lane);
   if (d.alpha == 0 && d.gamma == 0) { *code = kZero; *idx = 0; return; }
   if (is_good(d, csmix)) { *code = kGood; *idx = d.alpha; return; }
   for (uint32_t j0 = 0; j0 < bkt; j0 += 32) {
     const uint32_t j = j0 + lane;
-    bool good = false;
-    uint64_t a = 0;
-    if (j < bkt) {
-      const GsBucket b = ld_bucket_cg(col + j);
-      a = b.alpha;
-      good = is_good(b, csmix);
-    }
+    if (j0 > 0 && j < bkt) b = ld_bucket_cg(col + j);
+    const bool good = j < bkt && is_good(b, csmix);
     const uint32_t m = __ballot_sync(0xffffffffu, good);
     if (m) {
       *code = kGood;
-      *idx = __shfl_sync(0xffffffffu, a, __ffs(m) - 1);
+      *idx = __shfl_sync(0xffffffffu, b.alpha, __ffs(m) - 1);
       return;
     }
   }
@@ -163,9 +171,10 @@ struct BorArgs {
   uint32_t* size;              // [V]
   GsBucket* acc;               // [V][W]
   uint64_t* samp;              // [V] sampled edge of each root this round (global ids), ~0 = none
+  uint32_t* roots;             // [V] this round's roots, status[3] of them
   uint32_t* forest;            // [2 * forest_cap]
   uint32_t forest_cap;
-  uint32_t* status;            // [0] error bits [4] forest edges [5] active tenants [6,7] barrier
+  uint32_t* status;            // [0] error bits [3] roots [4] forest edges [5] active tenants [6,7] barrier
   uint32_t* tstate;            // [T][4]: done, modified this round, rounds, out of samples
 };
 
@@ -191,24 +200,30 @@ __device__ __forceinline__ void snapshot_done(const BorArgs& A, uint32_t* s_done
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
-  extern __shared__ uint32_t s_done[];  // [T]
+// Dynamic shared memory: the tenants' done flags (T words, padded to 16 bytes), then one staging
+// area of kAccRun x W buckets per warp.
+__global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* s_done = smem;
+  GsBucket* stage = reinterpret_cast<GsBucket*>(smem + ((A.T + 3u) & ~3u)) + (threadIdx.x >> 5) * kAccRun * A.W;
   uint32_t* err = A.status;
+  uint32_t* nroots_p = A.status + 3;
   uint32_t* bcount = A.status + 6;
   uint32_t* bgen = A.status + 7;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
-  const uint32_t gwarp = gtid >> 5, gwarps = gthreads >> 5;
+  const uint32_t gwarp = gtid >> 5, gwarps = gthreads >> 5, lane = lane_id();
   const uint32_t limit = A.V + 64;
+  const uint32_t span = A.V - A.vlo;
 
   for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.parent[v] = v;
+  if (gtid == 0) *nroots_p = 0;
   if (!grid_sync(bcount, bgen, err)) return;
 
   for (uint32_t round = 0; round < A.max_rounds; round++) {
     snapshot_done(A, s_done);
     if (round > 0) {
-      // ---- sizes of the round's components (frozen root set) ----
-      for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.size[v] = 0;
-      if (!grid_sync(bcount, bgen, err)) return;
+      // ---- sizes of the round's components (size[] was zeroed by the previous compress); the
+      //      first adder of each root appends it to the root list ----
       for (uint32_t base = A.vlo + blockIdx.x * blockDim.x; base < A.V; base += gthreads) {
         const uint32_t v = base + threadIdx.x;
         uint32_t r = 0xffffffffu;
@@ -217,124 +232,124 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
           if (!s_done[t]) r = __ldcg(&A.parent[v]);
         }
         const uint32_t peers = __match_any_sync(0xffffffffu, r);
-        if (r != 0xffffffffu && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&A.size[r], (uint32_t)__popc(peers));
+        bool fresh = false;
+        if (r != 0xffffffffu && lane == (uint32_t)(__ffs(peers) - 1))
+          fresh = atomicAdd(&A.size[r], (uint32_t)__popc(peers)) == 0u;
+        const uint32_t fm = __ballot_sync(0xffffffffu, fresh);
+        if (fm) {
+          uint32_t at = 0;
+          if (lane == (uint32_t)(__ffs(fm) - 1)) at = atomicAdd(nroots_p, (uint32_t)__popc(fm));
+          at = __shfl_sync(0xffffffffu, at, __ffs(fm) - 1);
+          if (fresh) A.roots[at + __popc(fm & ((1u << lane) - 1u))] = r;
+        }
       }
       if (!grid_sync(bcount, bgen, err)) return;
-      // ---- zero the accumulators of non-singleton components ----
-      for (uint32_t v = A.vlo + gwarp; v < A.V; v += gwarps) {
-        if (__ldcg(&A.size[v]) <= 1) continue;
-        GsBucket* row = A.acc + (size_t)v * A.W;
-        for (uint32_t j = lane_id(); j < A.W; j += 32) row[j] = GsBucket{0, 0};
-      }
-      if (!grid_sync(bcount, bgen, err)) return;
+
       // ---- accumulate column r + the deterministic bucket per component ----
-      // kAccUnroll vertices' loads are issued together, then folded into the run's accumulator in order
-      for (uint32_t start = A.vlo + gwarp * kAccRun; start < A.V; start += gwarps * kAccRun) {
-        const uint32_t end = min(A.V, start + kAccRun);
+      // Each warp owns a contiguous slice of vertices and walks it kAccRun at a time: the columns of
+      // the run's members are copied into shared memory with cp.async (all in flight together), then
+      // folded in vertex order into a register accumulator that is flushed with red.global.xor when
+      // the component changes.  A vertex whose root is another vertex is in a component of two or
+      // more, so only roots read their own size: no load hammers a giant component's root.
+      {
+        const uint32_t per = ((span + gwarps - 1) / gwarps + kAccRun - 1) / kAccRun * kAccRun;
+        const uint32_t w0 = A.vlo + min(span, gwarp * per), w1 = A.vlo + min(span, gwarp * per + per);
         uint32_t cur = 0xffffffffu, w = 0;
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
-        for (uint32_t v0 = start; v0 < end; v0 += kAccUnroll) {
-          uint32_t root[kAccUnroll], vt[kAccUnroll];
-#pragma unroll
-          for (int u = 0; u < kAccUnroll; u++) {
-            const uint32_t v = v0 + u;
-            root[u] = 0xffffffffu;
-            vt[u] = 0;
-            if (v < end) {
-              vt[u] = A.vtenant ? A.vtenant[v] : 0u;
-              if (!s_done[vt[u]]) root[u] = __ldcg(&A.parent[v]);
+        for (uint32_t start = w0; start < w1; start += kAccRun) {
+          const uint32_t n = min(kAccRun, w1 - start);
+          uint32_t rt = 0xffffffffu, tt = 0;
+          if (lane < n) {
+            const uint32_t v = start + lane;
+            tt = A.vtenant ? A.vtenant[v] : 0u;
+            if (!s_done[tt]) {
+              const uint32_t r = __ldcg(&A.parent[v]);
+              if (r != v || __ldcg(&A.size[v]) > 1u) rt = r;
             }
           }
-#pragma unroll
-          for (int u = 0; u < kAccUnroll; u++)
-            if (root[u] != 0xffffffffu && __ldcg(&A.size[root[u]]) <= 1) root[u] = 0xffffffffu;
-          uint64_t la[kAccUnroll][3], lg[kAccUnroll][3];
-          uint32_t lw[kAccUnroll];
-#pragma unroll
-          for (int u = 0; u < kAccUnroll; u++) {
-            lw[u] = 0;
-#pragma unroll
-            for (int k = 0; k < 3; k++) la[u][k] = lg[u][k] = 0;
-            if (root[u] == 0xffffffffu) continue;
-            const GsBorTenant& T = tenant_of(A, vt[u]);
-            const uint32_t bkt = T.bkt, nb = T.nb;
-            lw[u] = bkt + 1;
-            const GsBucket* base = A.sk + T.sk_off + (size_t)(v0 + u - T.vbase) * nb;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-              const uint32_t j = lane_id() + 32u * k;
-              if (j <= bkt) {
-                const GsBucket b = j < bkt ? base[(size_t)round * bkt + j] : base[nb - 1];
-                la[u][k] = b.alpha;
-                lg[u][k] = b.gamma;
-              }
-            }
+          const uint32_t live = __ballot_sync(0xffffffffu, rt != 0xffffffffu);
+          for (uint32_t m = live; m;) {
+            const uint32_t i = __ffs(m) - 1;
+            m &= m - 1;
+            const GsBorTenant& T = tenant_of(A, __shfl_sync(0xffffffffu, tt, i));
+            const GsBucket* vb = A.sk + T.sk_off + (size_t)(start + i - T.vbase) * T.nb;
+            for (uint32_t j = lane; j <= T.bkt; j += 32)
+              cp_async16(stage + i * A.W + j, j < T.bkt ? vb + (size_t)round * T.bkt + j : vb + (T.nb - 1));
           }
-#pragma unroll
-          for (int u = 0; u < kAccUnroll; u++) {
-            if (root[u] == 0xffffffffu) continue;
-            if (root[u] != cur) {
+          cp_async_wait_all();
+          __syncwarp();
+          for (uint32_t m = live; m;) {
+            const uint32_t i = __ffs(m) - 1;
+            m &= m - 1;
+            const uint32_t root = __shfl_sync(0xffffffffu, rt, i);
+            if (root != cur) {
               if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
-              cur = root[u];
-              w = lw[u];
+              cur = root;
+              w = tenant_of(A, __shfl_sync(0xffffffffu, tt, i)).bkt + 1;
 #pragma unroll
               for (int k = 0; k < 3; k++) a[k] = gm[k] = 0;
             }
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-              a[k] ^= la[u][k];
-              gm[k] ^= lg[u][k];
+              const uint32_t j = lane + 32u * k;
+              if (j < w) {
+                const GsBucket b = stage[i * A.W + j];
+                a[k] ^= b.alpha;
+                gm[k] ^= b.gamma;
+              }
             }
           }
+          __syncwarp();
         }
         if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
       }
       if (!grid_sync(bcount, bgen, err)) return;
     }
 
-    // ---- sample every root: one warp per root, the result to samp[root] ----
-    for (uint32_t v = A.vlo + gwarp; v < A.V; v += gwarps) {
+    // ---- sample every root into samp[root]: roots spread over the warps by list position ----
+    // The accumulator row of a sampled component is zeroed after reading, so every row is zero
+    // again when the round ends (and at the start of the next launch).
+    const uint32_t nroots = round == 0 ? span : ld_volatile(nroots_p);
+    for (uint32_t k = gwarp; k < nroots; k += gwarps) {
+      const uint32_t v = round == 0 ? A.vlo + k : __ldcg(&A.roots[k]);
       const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
       if (s_done[t]) continue;
-      uint32_t sz = 1;
-      if (round > 0) {
-        sz = __ldcg(&A.size[v]);
-        if (sz == 0) continue;  // not a root this round
-      }
+      const uint32_t sz = round == 0 ? 1u : __ldcg(&A.size[v]);
       const GsBorTenant& T = tenant_of(A, t);
       const uint32_t col = round == 0 ? T.round0_col : round;
+      GsBucket* acc = A.acc + (size_t)v * A.W;
       if (col >= T.ns) {  // OutOfSamplesException
-        if (lane_id() == 0) A.tstate[4 * t + 3] = 1u;
-        continue;
-      }
-      const GsBucket* own = A.sk + T.sk_off + (size_t)(v - T.vbase) * T.nb;
-      uint32_t code;
-      uint64_t idx;
-      if (sz > 1) {
-        const GsBucket* acc = A.acc + (size_t)v * A.W;
-        sample_warp(acc, acc + T.bkt, T.bkt, T.csmix, &code, &idx);
+        if (lane == 0) A.tstate[4 * t + 3] = 1u;
       } else {
-        sample_warp(own + (size_t)col * T.bkt, own + (T.nb - 1), T.bkt, T.csmix, &code, &idx);
-      }
-      if (lane_id() == 0) {
-        uint64_t e = ~0ull;
-        if (code == kFail) {
-          A.tstate[4 * t + 1] = 1u;
-        } else if (code == kGood) {
-          const uint32_t s = (uint32_t)(idx >> 32), d = (uint32_t)idx;
-          if (s < T.V && d < T.V && s != d)  // anything else is a checksum collision
-            e = ((uint64_t)(T.vbase + s) << 32) | (T.vbase + d);
+        const GsBucket* own = A.sk + T.sk_off + (size_t)(v - T.vbase) * T.nb;
+        uint32_t code;
+        uint64_t idx;
+        if (sz > 1) sample_warp(acc, acc + T.bkt, T.bkt, T.csmix, &code, &idx);
+        else sample_warp(own + (size_t)col * T.bkt, own + (T.nb - 1), T.bkt, T.csmix, &code, &idx);
+        if (lane == 0) {
+          uint64_t e = ~0ull;
+          if (code == kFail) {
+            A.tstate[4 * t + 1] = 1u;
+          } else if (code == kGood) {
+            const uint32_t s = (uint32_t)(idx >> 32), d = (uint32_t)idx;
+            if (s < T.V && d < T.V && s != d)  // anything else is a checksum collision
+              e = ((uint64_t)(T.vbase + s) << 32) | (T.vbase + d);
+          }
+          A.samp[v] = e;
         }
-        A.samp[v] = e;
+      }
+      if (sz > 1) {
+        __syncwarp();
+        for (uint32_t j = lane; j <= T.bkt; j += 32) acc[j] = GsBucket{0, 0};
       }
     }
     if (!grid_sync(bcount, bgen, err)) return;
 
     // ---- union the sampled edges: one thread per root, so many DSU walks are in flight ----
-    for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) {
+    for (uint32_t k = gtid; k < nroots; k += gthreads) {
+      const uint32_t v = round == 0 ? A.vlo + k : __ldcg(&A.roots[k]);
       const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
       if (s_done[t]) continue;
-      if (round > 0 && __ldcg(&A.size[v]) == 0) continue;
       const GsBorTenant& T = tenant_of(A, t);
       if ((round == 0 ? T.round0_col : round) >= T.ns) continue;
       const uint64_t e = __ldcg(&A.samp[v]);
@@ -342,20 +357,22 @@ __global__ void __launch_bounds__(256) k_boruvka(const BorArgs A) {
       const uint32_t gs = (uint32_t)(e >> 32), gd = (uint32_t)e;
       if (dsu_union(A.parent, gs, gd, limit, err)) {
         A.tstate[4 * t + 1] = 1u;
-        const uint32_t k = atomicAdd(&A.status[4], 1u);
-        if (k < A.forest_cap) {
-          A.forest[2 * k] = min(gs, gd);
-          A.forest[2 * k + 1] = max(gs, gd);
+        const uint32_t f = atomicAdd(&A.status[4], 1u);
+        if (f < A.forest_cap) {
+          A.forest[2 * f] = min(gs, gd);
+          A.forest[2 * f + 1] = max(gs, gd);
         }
       }
     }
     if (!grid_sync(bcount, bgen, err)) return;
 
-    // ---- compress ----
-    for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.parent[v] = dsu_find(A.parent, v, limit, err);
-    if (!grid_sync(bcount, bgen, err)) return;
-
-    // ---- per tenant: stop at the first unmodified round ----
+    // ---- compress, clear the sizes and the root list for the next round, and per tenant stop
+    //      at the first unmodified round (the modified flags were final at the last barrier) ----
+    for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) {
+      A.parent[v] = dsu_find(A.parent, v, limit, err);
+      A.size[v] = 0;
+    }
+    if (gtid == 0) *nroots_p = 0;
     for (uint32_t t = gtid; t < A.T; t += gthreads) {
       volatile uint32_t* ts = A.tstate + 4 * t;
       if (ts[0]) continue;
@@ -397,19 +414,32 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
   A.size = L.size;
   A.acc = L.acc;
   A.samp = L.samp;
+  A.roots = L.roots;
   A.forest = L.forest;
   A.forest_cap = L.forest_cap;
   A.status = L.status;
   A.tstate = L.tstate;
   int dev = 0;
   GS_CUDA_TRY(cudaGetDevice(&dev));
-  const size_t smem = (size_t)L.T * sizeof(uint32_t);
-  int per_sm = 0, sms = 0;
-  GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_boruvka, 256, smem));
-  GS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const int blocks = (per_sm > 0 ? per_sm : 1) * sms;  // every block co-resident: the cooperative-launch limit
+  const size_t smem = (size_t)((L.T + 3u) & ~3u) * sizeof(uint32_t) + (size_t)kWarps * kAccRun * L.W * sizeof(GsBucket);
+  // occupancy depends on the shared-memory size: cache it per (device, size)
+  struct Occ { size_t smem = 0; int blocks = 0; };
+  static Occ occ[64];
+  Occ& o = occ[dev < 64 ? dev : 63];
+  if (o.smem != smem) {
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_boruvka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, sms = 0;
+    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_boruvka, kThreads, smem));
+    GS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm < 1) {
+      gs_set_error("Boruvka kernel does not fit on an SM with " + std::to_string(smem) + " bytes of shared memory");
+      return GS_ERR_BAD_ARG;
+    }
+    o.smem = smem;
+    o.blocks = per_sm * sms;  // every block co-resident: the cooperative-launch limit
+  }
   void* args[] = {&A};
-  GS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_boruvka, dim3(blocks), dim3(256), args, smem, s));
+  GS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_boruvka, dim3(o.blocks), dim3(kThreads), args, smem, s));
   return GS_OK;
 }
 
@@ -436,11 +466,15 @@ gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStrea
   L.size = g->d_size;
   L.acc = g->d_acc;
   L.samp = g->d_samp;
+  L.roots = g->d_res;
   L.forest = g->d_forest;
   L.forest_cap = V;
   L.status = g->d_status;
   L.tstate = g->d_status + 8;
 
+  // the kernel expects all-zero accumulator rows and leaves them so when it runs to the end
+  if (g->acc_dirty) GS_CUDA_TRY(cudaMemsetAsync(g->d_acc, 0, (size_t)V * (bkt + 1) * sizeof(GsBucket), s));
+  g->acc_dirty = true;
   // status: everything zero except the count of tenants still running
   g->h_status[15] = 1;
   GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 16 * sizeof(uint32_t), s));
@@ -460,6 +494,7 @@ gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStrea
     gs_set_error("DSU walk exceeded its bound");
     return GS_ERR_INTERNAL;
   }
+  g->acc_dirty = false;
   if (st[8 + 3]) {
     gs_set_error("sketch ran out of samples after " + std::to_string(st[8 + 2]) + " Boruvka rounds");
     return GS_ERR_SKETCH_FAIL;

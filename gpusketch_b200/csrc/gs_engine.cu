@@ -250,10 +250,10 @@ gs_status gs_engine_tenant_bytes(uint32_t num_vertices, double sketches_factor, 
 gs_status gs_engine_create(const gs_engine_config* cfg, gs_engine** out) {
   if (!cfg || !out) { gs_set_error("gs_engine_create: null argument"); return GS_ERR_BAD_ARG; }
   *out = nullptr;
-  if (cfg->max_tenants < 1 || cfg->max_tenants > 65535 || cfg->max_vertices < 2 ||
+  if (cfg->max_tenants < 1 || cfg->max_tenants > 4096 || cfg->max_vertices < 2 ||
       cfg->max_vertices >= 0xffffffffu - 64 || cfg->max_tenant_vertices < 2 ||
       cfg->max_tenant_vertices > cfg->max_vertices || cfg->sketch_budget_bytes < sizeof(GsBucket)) {
-    gs_set_error("gs_engine_create: need 1 <= max_tenants <= 65535, 2 <= max_tenant_vertices <= max_vertices < 2^32 - 64 "
+    gs_set_error("gs_engine_create: need 1 <= max_tenants <= 4096, 2 <= max_tenant_vertices <= max_vertices < 2^32 - 64 "
                  "and a sketch budget");
     return GS_ERR_BAD_ARG;
   }
@@ -598,6 +598,9 @@ gs_status gs_engine_connected_components(gs_engine* e, const uint32_t* tenants, 
   GS_CUDA_TRY(cudaMemsetAsync(e->d_ncc, 0, (size_t)count * sizeof(uint32_t), s));
   GS_CUDA_TRY(cudaEventRecord(e->ev_tables, s));
 
+  if (g->acc_dirty)
+    GS_CUDA_TRY(cudaMemsetAsync(g->d_acc, 0, (size_t)e->max_vertices * e->W * sizeof(GsBucket), s));
+  g->acc_dirty = true;
   GsBorLaunch L;
   L.sk = g->d_sk;
   L.tenants = e->d_bor;
@@ -611,6 +614,7 @@ gs_status gs_engine_connected_components(gs_engine* e, const uint32_t* tenants, 
   L.size = g->d_size;
   L.acc = g->d_acc;
   L.samp = g->d_samp;
+  L.roots = g->d_res;
   L.forest = g->d_forest;
   L.forest_cap = e->max_vertices;
   L.status = e->d_qstatus;
@@ -629,6 +633,7 @@ gs_status gs_engine_connected_components(gs_engine* e, const uint32_t* tenants, 
   GS_CUDA_TRY(cudaStreamSynchronize(s));
   if (labels) GS_CUDA_TRY(cudaMemcpy(labels, g->d_res, total * sizeof(uint32_t), cudaMemcpyDeviceToHost));
   const uint32_t qerr = e->h_qstatus[0], ierr = g->h_status[0];
+  g->acc_dirty = (qerr & (GS_DEV_ERR_TIMEOUT | GS_DEV_ERR_DSU_LIMIT)) != 0;
   if (qerr & GS_DEV_ERR_TIMEOUT) {
     gs_set_error("a grid barrier of the Boruvka kernel gave up waiting");
     return GS_ERR_TIMEOUT;

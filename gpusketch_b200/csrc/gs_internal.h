@@ -79,6 +79,7 @@ struct gs_graph {
   uint32_t* d_res = nullptr;     // [V] sample result code
   uint64_t* d_samp = nullptr;    // [V] sampled edge id
   GsBucket* d_acc = nullptr;     // [V][bkt_per_col+1] merged column + deterministic bucket
+  bool acc_dirty = true;         // d_acc may hold non-zero rows (new, or a query ended early)
   uint32_t* d_forest = nullptr;  // [2*(V-1)] forest edges of the last Boruvka run
   uint32_t last_forest_edges = 0;
   uint32_t last_rounds = 0;
@@ -159,6 +160,7 @@ struct GsBorLaunch {
   uint32_t* size = nullptr;
   GsBucket* acc = nullptr;
   uint64_t* samp = nullptr;              // [V]
+  uint32_t* roots = nullptr;             // [V]
   uint32_t* forest = nullptr;
   uint32_t forest_cap = 0;
   uint32_t* status = nullptr;            // 8 words: [0] errors [4] forest edges [5] running tenants [6,7] barrier

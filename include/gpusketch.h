@@ -254,7 +254,7 @@ typedef struct gs_engine gs_engine;
 
 typedef struct gs_engine_config {
   uint64_t sketch_budget_bytes;  /* device arena for tenant sketches (the admission limit) */
-  uint32_t max_tenants;          /* tenant slots (1..65535) */
+  uint32_t max_tenants;          /* tenant slots (1..4096) */
   uint32_t max_vertices;         /* engine vertex space: total V over live tenants */
   uint32_t max_tenant_vertices;  /* largest V of one tenant (sizes the Boruvka scratch) */
   int32_t device;                /* CUDA device ordinal; < 0 = current device */
