@@ -46,6 +46,11 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default launch parameters")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target wall time of the CPU sample")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 256-stream batched engine comparison")
+    ap.add_argument("--no-served", action="store_true", help="skip the 64-tenant served trace")
+    ap.add_argument("--batched-streams", type=int, default=256)
+    ap.add_argument("--batched-phases", type=int, default=4)
+    ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request trace")
     return ap.parse_args()
 
 
@@ -211,6 +216,131 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, dev, steps, warmup):
+    """256 independent ER streams (seeds 0x5EED1000+i, V = round(2^U(8,14)), degree U(4,64), 10% churn)
+    in `phases` phases.  Engine: one gs_engine_phase per phase (device-resident slices of every stream,
+    then one Boruvka launch over all 256 tenants), recorded and launched as one CUDA graph.  Plain: the
+    single-graph path, one GraphSketch per stream, an ingest call and a connected_components() call per
+    stream per phase.  Both from device-resident records; wall time with the device idle on both sides
+    (each call returns after its work finished)."""
+    import numpy as np
+    import torch
+    import gpusketch_b200 as gs
+    from gpusketch_b200.autotune import autotune_engine
+    from gpusketch_b200.engine import SketchEngine, tenant_bytes
+    from gpusketch_b200.workloads import batched_streams, phase_slices
+
+    streams = batched_streams(args.batched_streams)
+    P = args.batched_phases
+    slices = phase_slices(streams, P)
+    total = sum(len(s.records) for s in streams)
+    d_phase, offs = [], []
+    for p in range(P):
+        parts = [s.records[lo:hi] for s, (lo, hi) in zip(streams, slices[p])]
+        offs.append(np.cumsum([0] + [len(x) for x in parts]).astype(np.uint64))
+        d_phase.append(torch.from_numpy(np.concatenate(parts).astype(np.int32)).to(dev))
+    budget = sum(tenant_bytes(s.V) for s in streams) + (64 << 20)
+    eng = SketchEngine(budget, len(streams), sum(s.V for s in streams), 1 << 14, device=dev.index)
+    ids = [eng.add_tenant(s.V, s.sketch_seed) for s in streams]
+    tune = autotune_engine(eng, ids, offs[0], d_phase[0])
+    for t in ids:
+        eng.clear_tenant(t)
+
+    def engine_step(graph=True):
+        for t in ids:
+            eng.clear_tenant(t)
+        out = []
+        for p in range(P):
+            out.append(eng.phase(ids, offs[p], d_phase[p], ids, cuda_graph=graph))
+        return out
+
+    def timed(fn, n):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = None
+        for _ in range(n):
+            res = fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / n, res
+
+    for _ in range(warmup):
+        engine_step()
+    eng_s, eng_res = timed(engine_step, steps)
+    eng.profile_enable(True)  # per-kernel-class split from the eager phases (graphs carry no timing events)
+    eager_s, eager_res = timed(lambda: engine_step(False), steps)
+    prof = eng.profile_read()
+    eng.profile_enable(False)
+    built, launched = eng.graph_stats()
+    used = eng.memory()[0]
+    eng.close()
+
+    handles = [gs.GraphSketch(s.V, s.sketch_seed, device=dev.index, max_batch_edges=1 << 20) for s in streams]
+
+    def plain_step():
+        for h in handles:
+            h.clear()
+        out = []
+        for p in range(P):
+            res = {}
+            d, o = d_phase[p], offs[p]
+            for k, h in enumerate(handles):
+                h.ingest_pairs(d[int(o[k]):int(o[k + 1])])
+                res[ids[k]] = h.connected_components()[1]
+            out.append(res)
+        return out
+
+    plain_step()
+    plain_s, plain_res = timed(plain_step, 1)
+    for h in handles:
+        h.close()
+    agree = all(plain_res[p][t] == eng_res[p][t][0] == eager_res[p][t][0] for p in range(P) for t in ids)
+    return {
+        "workload": f"batched_{len(streams)}_er_streams", "streams": len(streams), "phases": P,
+        "updates_per_step": total, "vertices": sum(s.V for s in streams), "sketch_bytes": used,
+        "engine_value": total / eng_s, "engine_eager_value": total / eager_s, "plain_value": total / plain_s,
+        "unit": UNIT, "speedup_vs_plain": plain_s / eng_s, "engine_ms_per_step": 1e3 * eng_s,
+        "engine_eager_ms_per_step": 1e3 * eager_s, "plain_ms_per_step": 1e3 * plain_s,
+        "engine_eager_split_ms_per_step": {k: prof[k] / steps for k in ("ingest_ms", "bucket_ms", "query_ms")},
+        "cuda_graphs": {"instantiated": built, "launched": launched},
+        "tuning": tune, "answers_agree": agree,
+        "timing": "wall clock per step around synchronous calls, device idle on both sides",
+    }
+
+
+def run_served(args, dev):
+    """64 tenants (V = round(2^U(10,16)), R-MAT records), Poisson arrivals (mean gap 2 ms), update
+    batches of round(2^U(10,20)) records from page-locked host buffers, 10% connectivity queries;
+    replayed in real time by the continuous-batching server and by the plain per-tenant server."""
+    import torch
+    from gpusketch_b200.engine import tenant_bytes
+    from gpusketch_b200.serve import PlainServer, SketchServer
+    from gpusketch_b200.workloads import served_trace
+
+    tr = served_trace(64, args.served_seconds)
+    need = sum(tenant_bytes(v) for v, _, _ in tr.tenants)
+    srv = SketchServer(tr, need + (256 << 20), device=dev.index)
+    host = srv.prepare()
+    payloads = [torch.from_numpy(a.astype("int32")).pin_memory() if a is not None else None for a in host]
+    srv.run(payloads, time_scale=0.05)  # warm-up pass 20x faster than real time; every tenant retires
+    st = srv.run(payloads)
+    srv.close()
+    plain = PlainServer(tr, device=dev.index)
+    pst = plain.run(payloads)
+    plain.close()
+
+    offered = sum(r.n for r in tr.requests if r.kind == "update")
+    return {
+        "workload": "served_64_tenants_rmat", "tenants": len(tr.tenants), "requests": len(tr.requests),
+        "queries": len(st.answers), "trace_seconds": args.served_seconds, "offered_updates": offered,
+        "query_latency_ms": st.latency_summary(), "updates_per_s": st.updates_per_s,
+        "plain_query_latency_ms": pst.latency_summary(), "plain_updates_per_s": pst.updates_per_s,
+        "ingest_calls": st.ingest_calls, "query_launches": st.query_launches,
+        "plain_ingest_calls": pst.ingest_calls, "wall_s": st.wall_s, "plain_wall_s": pst.wall_s,
+        "max_live_tenants": st.max_live_tenants, "sketch_bytes_needed": need,
+        "latency": "enqueue (trace arrival time) to answer, wall clock",
+    }
+
+
 def run_gs(args):
     import numpy as np
     import torch
@@ -337,6 +467,13 @@ def run_gs(args):
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference", "sample": f"failed: {exc}"}
 
     g.close()
+    del d_in
+    torch.cuda.empty_cache()
+    batched = served = None
+    if not args.no_batched:
+        batched = run_batched(args, dev, max(1, args.steps), max(1, args.warmup))
+    if not args.no_served:
+        served = run_served(args, dev)
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -351,7 +488,7 @@ def run_gs(args):
                    "sketch_bytes_per_vertex": Sv, "l2": "inputs larger than L2 (8 GiB of records per GPU)",
                    "parallelism": f"replicas x{world}", "tuning": tuning},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": prof["kernel_launches"],
-        "clocks": clocks, "kernel_split": split,
+        "clocks": clocks, "kernel_split": split, "batched": batched, "served": served,
     }
     if os.environ.get("GS_BENCH_TUNE_TABLE"):
         line["tune_table"] = tune_table

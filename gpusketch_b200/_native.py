@@ -21,6 +21,7 @@ GS_ERR_UPDATE_LOCKED = 6
 GS_ERR_IO = 7
 GS_ERR_INTERNAL = 8
 GS_ERR_NO_DEVICE = 9
+GS_PHASE_CUDA_GRAPH = 1
 
 STATUS_NAMES = {
     0: "GS_OK", 1: "GS_ERR_BAD_ARG", 2: "GS_ERR_CUDA", 3: "GS_ERR_OOM", 4: "GS_ERR_SKETCH_FAIL",
@@ -91,11 +92,15 @@ SIGNATURES = {
     "gs_engine_tenant_bytes": (C.c_int, [C.c_uint32, C.c_double, _U64P]),
     "gs_engine_add_tenant": (C.c_int, [_P, C.c_uint32, C.c_uint64, C.c_double, _U32P]),
     "gs_engine_remove_tenant": (C.c_int, [_P, C.c_uint32]),
+    "gs_engine_clear_tenant": (C.c_int, [_P, C.c_uint32]),
     "gs_engine_memory": (C.c_int, [_P, _U64P, _U64P, _U32P]),
     "gs_engine_set_stream": (C.c_int, [_P, _P]),
     "gs_engine_ingest": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_int, _P]),
+    "gs_engine_ingest_slices": (C.c_int, [_P, C.c_uint32, _P, _P, _P, _P]),
     "gs_engine_synchronize": (C.c_int, [_P]),
     "gs_engine_connected_components": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P]),
+    "gs_engine_phase": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, _P, C.c_int]),
+    "gs_engine_graph_stats": (C.c_int, [_P, _U64P, _U64P]),
     "gs_engine_tenant_geometry": (C.c_int, [_P, C.c_uint32, C.POINTER(GsGeometry)]),
     "gs_engine_download_sketches": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P]),
     "gs_engine_write_binary": (C.c_int, [_P, C.c_uint32, C.c_char_p]),

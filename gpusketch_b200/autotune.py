@@ -24,15 +24,23 @@ def _sig():
     return lib()
 
 
+def _fns(obj):
+    """(get, set) entry points for a GraphSketch or a SketchEngine handle."""
+    L = _sig()
+    if hasattr(obj, "phase"):
+        return L.gs_engine_get_tuning, L.gs_engine_set_tuning
+    return L.gs_get_tuning, L.gs_set_tuning
+
+
 def get_tuning(g) -> dict:
     t = GsTuning()
-    check(_sig().gs_get_tuning(g._h, C.byref(t)), "gs_get_tuning")
+    check(_fns(g)[0](g._h, C.byref(t)), "get_tuning")
     return {"chunk": t.chunk, "warps_per_block": t.warps_per_block, "reg_depth": t.reg_depth}
 
 
 def set_tuning(g, chunk: int, warps_per_block: int, reg_depth: int) -> None:
     t = GsTuning(chunk, warps_per_block, reg_depth, 0)
-    check(_sig().gs_set_tuning(g._h, C.byref(t)), "gs_set_tuning")
+    check(_fns(g)[1](g._h, C.byref(t)), "set_tuning")
 
 
 def autotune(g, sample_pairs, chunks=(256, 512, 1024, 2048, 4096), warps=(4, 8, 16), reg_depths=(1, 2),
@@ -58,4 +66,27 @@ def autotune(g, sample_pairs, chunks=(256, 512, 1024, 2048, 4096), warps=(4, 8, 
     g.profile_enable(False)
     set_tuning(g, *best)
     _CACHE[key] = best
+    return {"chunk": best[0], "warps_per_block": best[1], "reg_depth": best[2], "ingest_ms": best_ms / (2 * repeats)}
+
+
+def autotune_engine(e, slice_tenants, slice_offsets, pairs, chunks=(128, 256, 512, 1024), warps=(4, 8, 16),
+                    reg_depths=(1, 2), repeats: int = 1, table: list | None = None) -> dict:
+    """Engine variant: times the multi-tenant sketch update on one batch of device-resident slices
+    (ingested twice per candidate, so the tenants' sketches are unchanged) and applies the fastest.
+    Tile size = records per work item, vertices per block = warps per block (a warp owns one vertex
+    chunk), update-buffer depth = bucket depths kept in registers."""
+    best, best_ms = None, float("inf")
+    for chunk, w, r in itertools.product(chunks, warps, reg_depths):
+        set_tuning(e, chunk, w, r)
+        e.profile_enable(True)
+        for _ in range(repeats):
+            e.ingest(slice_tenants, slice_offsets, pairs)
+            e.ingest(slice_tenants, slice_offsets, pairs)
+        ms = e.profile_read()["ingest_ms"]
+        if table is not None:
+            table.append({"chunk": chunk, "warps_per_block": w, "reg_depth": r, "ingest_ms": ms / (2 * repeats)})
+        if ms < best_ms:
+            best, best_ms = (chunk, w, r), ms
+    e.profile_enable(False)
+    set_tuning(e, *best)
     return {"chunk": best[0], "warps_per_block": best[1], "reg_depth": best[2], "ingest_ms": best_ms / (2 * repeats)}

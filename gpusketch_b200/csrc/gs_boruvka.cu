@@ -110,6 +110,19 @@ __device__ __forceinline__ uint32_t dsu_find(uint32_t* parent, uint32_t x, uint3
   return x;
 }
 
+// Root of x without writing anything: the compress phase, where each parent[v] must have exactly
+// one writer (thread v).  A path-halving store from another thread could otherwise land after v's
+// root and leave v pointing at a non-root.
+__device__ __forceinline__ uint32_t dsu_root(const uint32_t* parent, uint32_t x, uint32_t limit, uint32_t* err) {
+  for (uint32_t it = 0; it < limit; it++) {
+    const uint32_t p = ld_volatile(parent + x);
+    if (p == x) return x;
+    x = p;
+  }
+  atomicOr(err, (uint32_t)GS_DEV_ERR_DSU_LIMIT);
+  return x;
+}
+
 // union of global vertices a, b; true when it joined two components
 __device__ __forceinline__ bool dsu_union(uint32_t* parent, uint32_t a, uint32_t b, uint32_t limit, uint32_t* err) {
   for (uint32_t it = 0; it < limit; it++) {
@@ -369,7 +382,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
     // ---- compress, clear the sizes and the root list for the next round, and per tenant stop
     //      at the first unmodified round (the modified flags were final at the last barrier) ----
     for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) {
-      A.parent[v] = dsu_find(A.parent, v, limit, err);
+      A.parent[v] = dsu_root(A.parent, v, limit, err);
       A.size[v] = 0;
     }
     if (gtid == 0) *nroots_p = 0;
@@ -438,8 +451,18 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
     o.smem = smem;
     o.blocks = per_sm * sms;  // every block co-resident: the cooperative-launch limit
   }
-  void* args[] = {&A};
-  GS_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_boruvka, dim3(o.blocks), dim3(kThreads), args, smem, s));
+  // cooperative through a launch attribute, so the launch can also be captured into a CUDA graph
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(o.blocks);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  GS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_boruvka, A));
   return GS_OK;
 }
 

@@ -556,7 +556,7 @@ extern "C" gs_status gs_set_tuning(gs_graph* g, const gs_tuning* t) {
 GsProfScope::GsProfScope(gs_graph* g_, int cls_, cudaStream_t s_, uint32_t launches) : g(g_), cls(cls_), s(s_) {
   g->prof_launches[cls] += launches;
   g->launches_total += launches;
-  if (!g->prof_on) return;
+  if (!g->prof_on || g->capturing) return;
   auto& ev = g->prof_ev[cls];
   const size_t i = g->prof_used[cls];
   if (ev.size() < 2 * (i + 1)) {

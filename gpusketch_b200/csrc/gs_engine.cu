@@ -163,15 +163,21 @@ struct gs_engine {
   uint32_t* d_q = nullptr;       // [2 * (max_tenants + 1)] query list, then label offsets
   uint32_t* h_q = nullptr;       // pinned mirror
   uint32_t* d_ncc = nullptr;     // [max_tenants + 1]
-  uint64_t* d_slices = nullptr;  // slice offsets of the current ingest call
-  uint64_t slices_cap = 0;
-  uint64_t* h_slices = nullptr;  // pinned mirror
-  uint64_t h_slices_cap = 0;
-  uint32_t* d_slice_ten = nullptr;
-  uint64_t slice_ten_cap = 0;
-  uint32_t* h_slice_ten = nullptr;
-  uint64_t h_slice_ten_cap = 0;
-  cudaEvent_t ev_tables = nullptr;  // the last upload from the pinned tables has been consumed
+  // Slice tables (record offsets and tenants) of an ingest, two sets so that one ingest's tables
+  // can be staged while the previous ingest's kernels still read theirs.
+  struct SliceTables {
+    uint64_t* d_off = nullptr;
+    uint64_t* h_off = nullptr;  // pinned
+    uint32_t* d_ten = nullptr;
+    uint32_t* h_ten = nullptr;  // pinned
+    uint64_t cap = 0;           // slices the buffers hold
+    cudaEvent_t ev_free = nullptr;  // the last kernel reading these tables has finished
+  } tabs[2];
+  uint64_t tab_next = 0;
+  uint64_t stage_next = 0;  // staging slot of the next ingest_slices chunk
+  cudaGraphExec_t phase_exec = nullptr;  // the last recorded phase, updated in place per phase
+  uint64_t phase_graphs_built = 0;
+  uint64_t phase_graph_launches = 0;
 };
 
 namespace {
@@ -180,13 +186,17 @@ void free_engine(gs_engine* e) {
   if (!e) return;
   if (e->g) gs_free_graph(e->g);
   cudaFree(e->d_ing); cudaFree(e->d_bor); cudaFree(e->d_vtenant); cudaFree(e->d_tstate);
-  cudaFree(e->d_qstatus); cudaFree(e->d_q); cudaFree(e->d_ncc); cudaFree(e->d_slices); cudaFree(e->d_slice_ten);
+  cudaFree(e->d_qstatus); cudaFree(e->d_q); cudaFree(e->d_ncc);
+  for (auto& tb : e->tabs) {
+    cudaFree(tb.d_off); cudaFree(tb.d_ten);
+    if (tb.h_off) cudaFreeHost(tb.h_off);
+    if (tb.h_ten) cudaFreeHost(tb.h_ten);
+    if (tb.ev_free) cudaEventDestroy(tb.ev_free);
+  }
   if (e->h_tstate) cudaFreeHost(e->h_tstate);
   if (e->h_qstatus) cudaFreeHost(e->h_qstatus);
   if (e->h_q) cudaFreeHost(e->h_q);
-  if (e->h_slices) cudaFreeHost(e->h_slices);
-  if (e->h_slice_ten) cudaFreeHost(e->h_slice_ten);
-  if (e->ev_tables) cudaEventDestroy(e->ev_tables);
+  if (e->phase_exec) cudaGraphExecDestroy(e->phase_exec);
   delete e;
 }
 
@@ -208,31 +218,180 @@ void refresh_bounds(gs_engine* e) {
   e->g->ten_min_bkt = min_bkt == 0xffffffffu ? 64u : min_bkt;
 }
 
-// Host slice tables -> device, through pinned buffers reused once the previous upload landed.
-gs_status upload_slices(gs_engine* e, const uint32_t* sten, const uint64_t* soff, uint32_t ns, cudaStream_t s) {
-  GS_CUDA_TRY(cudaEventSynchronize(e->ev_tables));
-  GS_TRY(grow_pinned(&e->h_slices, &e->h_slices_cap, (uint64_t)ns + 1));
-  GS_TRY(grow_pinned(&e->h_slice_ten, &e->h_slice_ten_cap, (uint64_t)ns));
-  GS_TRY(grow_device(&e->d_slices, &e->slices_cap, (uint64_t)ns + 1));
-  GS_TRY(grow_device(&e->d_slice_ten, &e->slice_ten_cap, (uint64_t)ns));
-  std::memcpy(e->h_slices, soff, ((size_t)ns + 1) * sizeof(uint64_t));
-  std::memcpy(e->h_slice_ten, sten, (size_t)ns * sizeof(uint32_t));
-  GS_CUDA_TRY(cudaMemcpyAsync(e->d_slices, e->h_slices, ((size_t)ns + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-  GS_CUDA_TRY(cudaMemcpyAsync(e->d_slice_ten, e->h_slice_ten, (size_t)ns * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  GS_CUDA_TRY(cudaEventRecord(e->ev_tables, s));
-  return GS_OK;
-}
-
 gs_status globalize(gs_engine* e, const uint32_t* in, uint32_t* out, uint64_t first, uint64_t m, uint32_t ns,
-                    cudaStream_t s) {
+                    const gs_engine::SliceTables& tb, cudaStream_t s) {
   const uint64_t want = (m + 255) / 256;
   const int grid = (int)std::min<uint64_t>(std::max<uint64_t>(want, 1), (uint64_t)e->g->num_sms * 16);
   {
     GsProfScope ps(e->g, GS_PROF_BUCKET, s, 1);
     k_globalize<<<grid, 256, 0, s>>>(reinterpret_cast<const uint2*>(in), reinterpret_cast<uint2*>(out), first, m,
-                                     e->d_slices, e->d_slice_ten, ns, e->d_ing, e->max_tenants, e->g->d_status);
+                                     tb.d_off, tb.d_ten, ns, e->d_ing, e->max_tenants, e->g->d_status);
   }
   GS_CUDA_TRY(cudaGetLastError());
+  return GS_OK;
+}
+
+struct QueryPlan {
+  std::vector<uint8_t> seen;
+  uint32_t vlo = 0xffffffffu, vhi = 0, max_rounds = 0;
+  uint64_t total = 0, maxv = 0;
+};
+
+gs_status plan_query(const gs_engine* e, const uint32_t* tenants, uint32_t count, QueryPlan* qp) {
+  if (count > e->max_tenants) { gs_set_error("engine query: too many tenants"); return GS_ERR_BAD_ARG; }
+  qp->seen.assign(e->max_tenants, 0);
+  for (uint32_t i = 0; i < count; i++) {
+    const uint32_t t = tenants[i];
+    if (!tenant_ok(e, t) || qp->seen[t]) {
+      gs_set_error("engine query: tenant " + std::to_string(t) + " is not live or listed twice");
+      return GS_ERR_BAD_ARG;
+    }
+    qp->seen[t] = 1;
+    const EngTenant& T = e->ten[t];
+    qp->vlo = std::min(qp->vlo, T.vbase);
+    qp->vhi = std::max(qp->vhi, T.vbase + T.V);
+    qp->max_rounds = std::max(qp->max_rounds, T.geom.num_samples);
+    qp->total += T.V;
+    qp->maxv = std::max<uint64_t>(qp->maxv, T.V);
+  }
+  return GS_OK;
+}
+
+gs_status check_slices(const gs_engine* e, const uint32_t* sten, const uint64_t* soff, uint32_t ns) {
+  for (uint32_t i = 0; i < ns; i++) {
+    if (soff[i + 1] < soff[i]) {
+      gs_set_error("engine ingest: slice offsets must not decrease");
+      return GS_ERR_BAD_ARG;
+    }
+    if (!tenant_ok(e, sten[i])) {
+      gs_set_error("engine ingest: slice " + std::to_string(i) + " names tenant " + std::to_string(sten[i]) +
+                   ", which is not live");
+      return GS_ERR_BAD_ARG;
+    }
+  }
+  return GS_OK;
+}
+
+// Host slice tables -> the pinned buffers of `tb` (whose previous reader has finished).
+gs_status stage_slices(gs_engine::SliceTables& tb, const uint32_t* sten, const uint64_t* soff, uint32_t ns) {
+  if (tb.cap < (uint64_t)ns + 1) {
+    cudaFree(tb.d_off); cudaFree(tb.d_ten);
+    if (tb.h_off) cudaFreeHost(tb.h_off);
+    if (tb.h_ten) cudaFreeHost(tb.h_ten);
+    tb.d_off = nullptr; tb.d_ten = nullptr; tb.h_off = nullptr; tb.h_ten = nullptr; tb.cap = 0;
+    const uint64_t cap = std::max<uint64_t>(2 * ((uint64_t)ns + 1), 64);
+    GS_CUDA_TRY(cudaMalloc(&tb.d_off, cap * sizeof(uint64_t)));
+    GS_CUDA_TRY(cudaMalloc(&tb.d_ten, cap * sizeof(uint32_t)));
+    GS_CUDA_TRY(cudaMallocHost(&tb.h_off, cap * sizeof(uint64_t)));
+    GS_CUDA_TRY(cudaMallocHost(&tb.h_ten, cap * sizeof(uint32_t)));
+    tb.cap = cap;
+  }
+  if (soff) std::memcpy(tb.h_off, soff, ((size_t)ns + 1) * sizeof(uint64_t));
+  if (sten) std::memcpy(tb.h_ten, sten, (size_t)ns * sizeof(uint32_t));
+  return GS_OK;
+}
+
+gs_status copy_slices(const gs_engine::SliceTables& tb, uint32_t ns, cudaStream_t s) {
+  GS_CUDA_TRY(cudaMemcpyAsync(tb.d_off, tb.h_off, ((size_t)ns + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  GS_CUDA_TRY(cudaMemcpyAsync(tb.d_ten, tb.h_ten, (size_t)ns * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  return GS_OK;
+}
+
+// Queues one multi-tenant Boruvka launch and the read-back of its results into pinned memory.
+// The pinned query tables must not be read by queued work any more.
+gs_status enqueue_query(gs_engine* e, const QueryPlan& qp, const uint32_t* tenants, uint32_t count, cudaStream_t s) {
+  gs_graph* g = e->g;
+  const uint32_t T1 = e->max_tenants + 1;
+  // every tenant done except the listed ones; the idle slot stays done
+  for (uint32_t t = 0; t < T1; t++) {
+    e->h_tstate[4 * t] = t < e->max_tenants && qp.seen[t] ? 0u : 1u;
+    e->h_tstate[4 * t + 1] = e->h_tstate[4 * t + 2] = e->h_tstate[4 * t + 3] = 0u;
+  }
+  std::memset(e->h_qstatus, 0, 16 * sizeof(uint32_t));
+  e->h_qstatus[5] = count;
+  uint32_t off = 0;
+  for (uint32_t i = 0; i < count; i++) {
+    e->h_q[i] = tenants[i];
+    e->h_q[T1 + i] = off;
+    off += e->ten[tenants[i]].V;
+  }
+  if (g->acc_dirty)
+    GS_CUDA_TRY(cudaMemsetAsync(g->d_acc, 0, (size_t)e->max_vertices * e->W * sizeof(GsBucket), s));
+  g->acc_dirty = true;
+  GS_CUDA_TRY(cudaMemcpyAsync(e->d_tstate, e->h_tstate, (size_t)T1 * 4 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  GS_CUDA_TRY(cudaMemcpyAsync(e->d_qstatus, e->h_qstatus, 16 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  GS_CUDA_TRY(cudaMemcpyAsync(e->d_q, e->h_q, (size_t)2 * T1 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  GS_CUDA_TRY(cudaMemsetAsync(e->d_ncc, 0, (size_t)count * sizeof(uint32_t), s));
+
+  GsBorLaunch L;
+  L.sk = g->d_sk;
+  L.tenants = e->d_bor;
+  L.vtenant = e->d_vtenant;
+  L.T = T1;
+  L.vlo = qp.vlo;
+  L.V = qp.vhi;
+  L.W = e->W;
+  L.max_rounds = qp.max_rounds;
+  L.parent = g->d_parent;
+  L.size = g->d_size;
+  L.acc = g->d_acc;
+  L.samp = g->d_samp;
+  L.roots = g->d_res;
+  L.forest = g->d_forest;
+  L.forest_cap = e->max_vertices;
+  L.status = e->d_qstatus;
+  L.tstate = e->d_tstate;
+  {
+    GsProfScope ps(g, GS_PROF_QUERY, s, 2);
+    GS_TRY(gs_boruvka_launch(L, s));
+    const dim3 grid((unsigned)std::min<uint64_t>((qp.maxv + 255) / 256, 64), count);
+    k_gather_labels<<<grid, 256, 0, s>>>(g->d_parent, e->d_q, e->d_q + T1, e->d_bor, g->d_res, e->d_ncc);
+    GS_CUDA_TRY(cudaGetLastError());
+  }
+  GS_CUDA_TRY(cudaMemcpyAsync(e->h_qstatus, e->d_qstatus, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GS_CUDA_TRY(cudaMemcpyAsync(e->h_tstate, e->d_tstate, (size_t)T1 * 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GS_CUDA_TRY(cudaMemcpyAsync(e->h_q, e->d_ncc, (size_t)count * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  return GS_OK;
+}
+
+// After the queued query finished: error words, per-tenant results, labels.
+gs_status finish_query(gs_engine* e, const QueryPlan& qp, const uint32_t* tenants, uint32_t count, uint32_t* labels,
+                       uint32_t* num_cc, uint32_t* rounds) {
+  gs_graph* g = e->g;
+  cudaStream_t s = g->stream;
+  if (labels) GS_CUDA_TRY(cudaMemcpy(labels, g->d_res, qp.total * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  const uint32_t qerr = e->h_qstatus[0], ierr = g->h_status[0];
+  g->acc_dirty = (qerr & (GS_DEV_ERR_TIMEOUT | GS_DEV_ERR_DSU_LIMIT)) != 0;
+  if (qerr & GS_DEV_ERR_TIMEOUT) {
+    gs_set_error("a grid barrier of the Boruvka kernel gave up waiting");
+    return GS_ERR_TIMEOUT;
+  }
+  if (qerr & GS_DEV_ERR_DSU_LIMIT) {
+    gs_set_error("DSU walk exceeded its bound");
+    return GS_ERR_INTERNAL;
+  }
+  std::string oos;
+  for (uint32_t i = 0; i < count; i++) {
+    const uint32_t* ts = e->h_tstate + 4 * tenants[i];
+    if (num_cc) num_cc[i] = e->h_q[i];
+    if (rounds) rounds[i] = ts[2];
+    if (ts[3]) oos += (oos.empty() ? "" : ", ") + std::to_string(tenants[i]);
+  }
+  if (ierr) {
+    GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, sizeof(uint32_t), s));
+    GS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (ierr & GS_DEV_ERR_VERTEX_RANGE) {
+      gs_set_error("an edge record named a vertex id >= its tenant's num_vertices; those records were skipped");
+      return GS_ERR_BAD_ARG;
+    }
+    gs_set_error("device consistency check failed (bits " + std::to_string(ierr) + ")");
+    return GS_ERR_INTERNAL;
+  }
+  if (!oos.empty()) {
+    gs_set_error("sketches ran out of samples for tenant(s) " + oos);
+    return GS_ERR_SKETCH_FAIL;
+  }
   return GS_OK;
 }
 
@@ -329,10 +488,14 @@ gs_status gs_engine_create(const gs_engine_config* cfg, gs_engine** out) {
   GS_CUDA_TRY(cudaMalloc(&e->d_q, (size_t)2 * T1 * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMallocHost(&e->h_q, (size_t)2 * T1 * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMalloc(&e->d_ncc, (size_t)T1 * sizeof(uint32_t)));
-  GS_CUDA_TRY(cudaEventCreateWithFlags(&e->ev_tables, cudaEventDisableTiming));
+  for (auto& tb : e->tabs) GS_CUDA_TRY(cudaEventCreateWithFlags(&tb.ev_free, cudaEventDisableTiming));
   g->d_vtenant = e->d_vtenant;
   g->d_ten = e->d_ing;
   refresh_bounds(e.get());
+  // staging and bucketing scratch for a full batch are allocated now, so that serving allocates
+  // nothing once it has started
+  GS_TRY(gs_ensure_pair_staging(g));
+  GS_TRY(gs_reserve_ingest(g, g->max_batch_edges));
   GS_CUDA_TRY(cudaStreamSynchronize(g->stream));
   *out = e.release();
   return GS_OK;
@@ -453,6 +616,14 @@ gs_status gs_engine_remove_tenant(gs_engine* e, uint32_t tenant) {
   return GS_OK;
 }
 
+gs_status gs_engine_clear_tenant(gs_engine* e, uint32_t tenant) {
+  if (!e || !tenant_ok(e, tenant)) { gs_set_error("gs_engine_clear_tenant: no such tenant"); return GS_ERR_BAD_ARG; }
+  GS_ENGINE_GUARD(e);
+  const EngTenant& T = e->ten[tenant];
+  GS_CUDA_TRY(cudaMemsetAsync(e->g->d_sk + T.sk_off, 0, T.buckets * sizeof(GsBucket), e->g->stream));
+  return GS_OK;
+}
+
 gs_status gs_engine_memory(const gs_engine* e, uint64_t* used, uint64_t* capacity, uint32_t* live_tenants) {
   if (!e) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
   if (used) *used = e->used_bytes;
@@ -473,17 +644,7 @@ gs_status gs_engine_ingest(gs_engine* e, const uint32_t* slice_tenants, const ui
     return GS_ERR_BAD_ARG;
   }
   if (num_slices == 0) return GS_OK;
-  for (uint32_t i = 0; i < num_slices; i++) {
-    if (slice_offsets[i + 1] < slice_offsets[i]) {
-      gs_set_error("gs_engine_ingest: slice offsets must not decrease");
-      return GS_ERR_BAD_ARG;
-    }
-    if (!tenant_ok(e, slice_tenants[i])) {
-      gs_set_error("gs_engine_ingest: slice " + std::to_string(i) + " names tenant " +
-                   std::to_string(slice_tenants[i]) + ", which is not live");
-      return GS_ERR_BAD_ARG;
-    }
-  }
+  GS_TRY(check_slices(e, slice_tenants, slice_offsets, num_slices));
   const uint64_t first = slice_offsets[0], n = slice_offsets[num_slices] - first;
   if (n == 0) return GS_OK;
   if (!pairs) { gs_set_error("gs_engine_ingest: null pairs"); return GS_ERR_BAD_ARG; }
@@ -492,7 +653,10 @@ gs_status gs_engine_ingest(gs_engine* e, const uint32_t* slice_tenants, const ui
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
   g->labels_valid = false;
   GS_TRY(gs_ensure_pair_staging(g));
-  GS_TRY(upload_slices(e, slice_tenants, slice_offsets, num_slices, s));
+  gs_engine::SliceTables& tb = e->tabs[e->tab_next++ & 1];
+  GS_CUDA_TRY(cudaEventSynchronize(tb.ev_free));
+  GS_TRY(stage_slices(tb, slice_tenants, slice_offsets, num_slices));
+  GS_TRY(copy_slices(tb, num_slices, s));
   const uint64_t cap = g->pairs_cap;
 
   cudaPointerAttributes attr{};
@@ -508,7 +672,7 @@ gs_status gs_engine_ingest(gs_engine* e, const uint32_t* slice_tenants, const ui
     GS_CUDA_TRY(cudaEventSynchronize(g->ev_done[slot]));
     const uint32_t* src = pairs + 2 * (first + done);
     if (pairs_on_device) {
-      GS_TRY(globalize(e, src, dslot, first + done, m, num_slices, s));
+      GS_TRY(globalize(e, src, dslot, first + done, m, num_slices, tb, s));
     } else {
       if (!pinned) {
         std::memcpy(hp + (size_t)slot * cap * 2, src, (size_t)m * 2 * sizeof(uint32_t));
@@ -517,13 +681,98 @@ gs_status gs_engine_ingest(gs_engine* e, const uint32_t* slice_tenants, const ui
       GS_CUDA_TRY(cudaMemcpyAsync(dslot, src, (size_t)m * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, g->copy_stream));
       GS_CUDA_TRY(cudaEventRecord(g->ev_copy[slot], g->copy_stream));
       GS_CUDA_TRY(cudaStreamWaitEvent(s, g->ev_copy[slot], 0));
-      GS_TRY(globalize(e, dslot, dslot, first + done, m, num_slices, s));
+      GS_TRY(globalize(e, dslot, dslot, first + done, m, num_slices, tb, s));
     }
     GS_TRY(gs_ingest_device_pairs(g, dslot, m, -1, s));
     GS_CUDA_TRY(cudaEventRecord(g->ev_done[slot], s));
     done += m;
   }
+  GS_CUDA_TRY(cudaEventRecord(tb.ev_free, s));
   if (!pairs_on_device) GS_CUDA_TRY(cudaStreamSynchronize(g->copy_stream));
+  if (s != g->stream) {
+    GS_CUDA_TRY(cudaEventRecord(g->ev_order, s));
+    GS_CUDA_TRY(cudaStreamWaitEvent(g->stream, g->ev_order, 0));
+  }
+  return GS_OK;
+}
+
+gs_status gs_engine_ingest_slices(gs_engine* e, uint32_t num_slices, const uint32_t* slice_tenants,
+                                  const uint64_t* slice_counts, const uint32_t* const* slice_pairs, void* stream) {
+  if (!e || (num_slices && (!slice_tenants || !slice_counts || !slice_pairs))) {
+    gs_set_error("gs_engine_ingest_slices: null argument");
+    return GS_ERR_BAD_ARG;
+  }
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < num_slices; i++) {
+    if (!tenant_ok(e, slice_tenants[i])) {
+      gs_set_error("gs_engine_ingest_slices: slice " + std::to_string(i) + " names tenant " +
+                   std::to_string(slice_tenants[i]) + ", which is not live");
+      return GS_ERR_BAD_ARG;
+    }
+    if (slice_counts[i] && !slice_pairs[i]) {
+      gs_set_error("gs_engine_ingest_slices: null records of slice " + std::to_string(i));
+      return GS_ERR_BAD_ARG;
+    }
+    total += slice_counts[i];
+  }
+  if (total == 0) return GS_OK;
+  GS_ENGINE_GUARD(e);
+  gs_graph* g = e->g;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : g->stream;
+  g->labels_valid = false;
+  GS_TRY(gs_ensure_pair_staging(g));
+  const uint64_t cap = g->pairs_cap;
+  uint32_t* hp = static_cast<uint32_t*>(g->h_pin);
+  bool direct = false;  // some slice was copied straight from caller memory
+  uint32_t si = 0;
+  uint64_t so = 0;  // records of slice si already staged
+  while (si < num_slices) {
+    // one staging chunk: whole slices (the last one possibly split) up to `cap` records
+    const int slot = (int)(e->stage_next++ & 1);
+    gs_engine::SliceTables& tb = e->tabs[slot];
+    GS_CUDA_TRY(cudaEventSynchronize(g->ev_done[slot]));
+    GS_CUDA_TRY(cudaEventSynchronize(tb.ev_free));
+    uint32_t* dslot = g->d_pairs + (size_t)slot * cap * 2;
+    uint32_t* hslot = hp + (size_t)slot * cap * 2;
+    uint64_t m = 0;
+    uint32_t np = 0;
+    std::vector<uint64_t> offs{0};
+    std::vector<uint32_t> tens;
+    while (si < num_slices && m < cap) {
+      const uint64_t take = std::min(slice_counts[si] - so, cap - m);
+      if (take) {
+        const uint32_t* src = slice_pairs[si] + 2 * so;
+        cudaPointerAttributes attr{};
+        const bool pinned = cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (!pinned) {
+          std::memcpy(hslot + 2 * m, src, (size_t)take * 2 * sizeof(uint32_t));
+          src = hslot + 2 * m;
+        } else {
+          direct = true;
+        }
+        GS_CUDA_TRY(cudaMemcpyAsync(dslot + 2 * m, src, (size_t)take * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                    g->copy_stream));
+        tens.push_back(slice_tenants[si]);
+        m += take;
+        offs.push_back(m);
+        np++;
+      }
+      so += take;
+      if (so == slice_counts[si]) { si++; so = 0; }
+    }
+    if (np == 0) continue;
+    GS_TRY(stage_slices(tb, tens.data(), offs.data(), np));
+    GS_TRY(copy_slices(tb, np, g->copy_stream));
+    GS_CUDA_TRY(cudaEventRecord(g->ev_copy[slot], g->copy_stream));
+    GS_CUDA_TRY(cudaStreamWaitEvent(s, g->ev_copy[slot], 0));
+    GS_TRY(globalize(e, dslot, dslot, 0, m, np, tb, s));
+    GS_TRY(gs_ingest_device_pairs(g, dslot, m, -1, s));
+    GS_CUDA_TRY(cudaEventRecord(g->ev_done[slot], s));
+    GS_CUDA_TRY(cudaEventRecord(tb.ev_free, s));
+  }
+  // caller memory read in place must have landed before the caller may reuse it
+  if (direct) GS_CUDA_TRY(cudaStreamSynchronize(g->copy_stream));
   if (s != g->stream) {
     GS_CUDA_TRY(cudaEventRecord(g->ev_order, s));
     GS_CUDA_TRY(cudaStreamWaitEvent(g->stream, g->ev_order, 0));
@@ -555,114 +804,108 @@ gs_status gs_engine_connected_components(gs_engine* e, const uint32_t* tenants, 
                                          uint32_t* num_cc, uint32_t* rounds) {
   if (!e || (count && !tenants)) { gs_set_error("gs_engine_connected_components: null argument"); return GS_ERR_BAD_ARG; }
   if (count == 0) return GS_OK;
-  if (count > e->max_tenants) { gs_set_error("gs_engine_connected_components: too many tenants"); return GS_ERR_BAD_ARG; }
-  std::vector<uint8_t> seen(e->max_tenants, 0);
-  uint32_t vlo = 0xffffffffu, vhi = 0, max_rounds = 0;
-  uint64_t total = 0, maxv = 0;
-  for (uint32_t i = 0; i < count; i++) {
-    const uint32_t t = tenants[i];
-    if (!tenant_ok(e, t) || seen[t]) {
-      gs_set_error("gs_engine_connected_components: tenant " + std::to_string(t) + " is not live or listed twice");
-      return GS_ERR_BAD_ARG;
-    }
-    seen[t] = 1;
-    const EngTenant& T = e->ten[t];
-    vlo = std::min(vlo, T.vbase);
-    vhi = std::max(vhi, T.vbase + T.V);
-    max_rounds = std::max(max_rounds, T.geom.num_samples);
-    total += T.V;
-    maxv = std::max<uint64_t>(maxv, T.V);
-  }
+  QueryPlan qp;
+  GS_TRY(plan_query(e, tenants, count, &qp));
   GS_ENGINE_GUARD(e);
   gs_graph* g = e->g;
   cudaStream_t s = g->stream;
-  g->labels_valid = false;
-  const uint32_t T1 = e->max_tenants + 1;
-  // every tenant done except the listed ones; the idle slot stays done
-  GS_CUDA_TRY(cudaEventSynchronize(e->ev_tables));
-  for (uint32_t t = 0; t < T1; t++) {
-    e->h_tstate[4 * t] = t < e->max_tenants && seen[t] ? 0u : 1u;
-    e->h_tstate[4 * t + 1] = e->h_tstate[4 * t + 2] = e->h_tstate[4 * t + 3] = 0u;
-  }
-  std::memset(e->h_qstatus, 0, 16 * sizeof(uint32_t));
-  e->h_qstatus[5] = count;
-  uint32_t acc_off = 0;
-  for (uint32_t i = 0; i < count; i++) {
-    e->h_q[i] = tenants[i];
-    e->h_q[T1 + i] = acc_off;
-    acc_off += e->ten[tenants[i]].V;
-  }
-  GS_CUDA_TRY(cudaMemcpyAsync(e->d_tstate, e->h_tstate, (size_t)T1 * 4 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  GS_CUDA_TRY(cudaMemcpyAsync(e->d_qstatus, e->h_qstatus, 16 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  GS_CUDA_TRY(cudaMemcpyAsync(e->d_q, e->h_q, (size_t)2 * T1 * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  GS_CUDA_TRY(cudaMemsetAsync(e->d_ncc, 0, (size_t)count * sizeof(uint32_t), s));
-  GS_CUDA_TRY(cudaEventRecord(e->ev_tables, s));
-
-  if (g->acc_dirty)
-    GS_CUDA_TRY(cudaMemsetAsync(g->d_acc, 0, (size_t)e->max_vertices * e->W * sizeof(GsBucket), s));
-  g->acc_dirty = true;
-  GsBorLaunch L;
-  L.sk = g->d_sk;
-  L.tenants = e->d_bor;
-  L.vtenant = e->d_vtenant;
-  L.T = T1;
-  L.vlo = vlo;
-  L.V = vhi;
-  L.W = e->W;
-  L.max_rounds = max_rounds;
-  L.parent = g->d_parent;
-  L.size = g->d_size;
-  L.acc = g->d_acc;
-  L.samp = g->d_samp;
-  L.roots = g->d_res;
-  L.forest = g->d_forest;
-  L.forest_cap = e->max_vertices;
-  L.status = e->d_qstatus;
-  L.tstate = e->d_tstate;
-  {
-    GsProfScope ps(g, GS_PROF_QUERY, s, 2);
-    GS_TRY(gs_boruvka_launch(L, s));
-    const dim3 grid((unsigned)std::min<uint64_t>((maxv + 255) / 256, 64), count);
-    k_gather_labels<<<grid, 256, 0, s>>>(g->d_parent, e->d_q, e->d_q + T1, e->d_bor, g->d_res, e->d_ncc);
-    GS_CUDA_TRY(cudaGetLastError());
-  }
-  GS_CUDA_TRY(cudaMemcpyAsync(e->h_qstatus, e->d_qstatus, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  GS_CUDA_TRY(cudaMemcpyAsync(e->h_tstate, e->d_tstate, (size_t)T1 * 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  GS_CUDA_TRY(cudaMemcpyAsync(e->h_q, e->d_ncc, (size_t)count * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GS_TRY(enqueue_query(e, qp, tenants, count, s));
   GS_CUDA_TRY(cudaStreamSynchronize(s));
-  if (labels) GS_CUDA_TRY(cudaMemcpy(labels, g->d_res, total * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-  const uint32_t qerr = e->h_qstatus[0], ierr = g->h_status[0];
-  g->acc_dirty = (qerr & (GS_DEV_ERR_TIMEOUT | GS_DEV_ERR_DSU_LIMIT)) != 0;
-  if (qerr & GS_DEV_ERR_TIMEOUT) {
-    gs_set_error("a grid barrier of the Boruvka kernel gave up waiting");
-    return GS_ERR_TIMEOUT;
+  return finish_query(e, qp, tenants, count, labels, num_cc, rounds);
+}
+
+gs_status gs_engine_phase(gs_engine* e, const uint32_t* slice_tenants, const uint64_t* slice_offsets,
+                          uint32_t num_slices, const uint32_t* pairs, const uint32_t* query_tenants,
+                          uint32_t query_count, uint32_t* num_cc, uint32_t* rounds, int flags) {
+  if (!e || (num_slices && (!slice_tenants || !slice_offsets || !pairs)) || (query_count && !query_tenants)) {
+    gs_set_error("gs_engine_phase: null argument");
+    return GS_ERR_BAD_ARG;
   }
-  if (qerr & GS_DEV_ERR_DSU_LIMIT) {
-    gs_set_error("DSU walk exceeded its bound");
-    return GS_ERR_INTERNAL;
+  GS_TRY(check_slices(e, slice_tenants, slice_offsets, num_slices));
+  const uint64_t first = num_slices ? slice_offsets[0] : 0;
+  const uint64_t n = num_slices ? slice_offsets[num_slices] - first : 0;
+  QueryPlan qp;
+  if (query_count) GS_TRY(plan_query(e, query_tenants, query_count, &qp));
+  GS_ENGINE_GUARD(e);
+  gs_graph* g = e->g;
+  cudaStream_t s = g->stream;
+  GS_TRY(gs_ensure_pair_staging(g));
+  if (n > g->pairs_cap) {
+    gs_set_error("gs_engine_phase: at most " + std::to_string(g->pairs_cap) + " records per phase, got " +
+                 std::to_string(n));
+    return GS_ERR_BAD_ARG;
   }
-  std::string oos;
-  for (uint32_t i = 0; i < count; i++) {
-    const uint32_t* ts = e->h_tstate + 4 * tenants[i];
-    if (num_cc) num_cc[i] = e->h_q[i];
-    if (rounds) rounds[i] = ts[2];
-    if (ts[3]) oos += (oos.empty() ? "" : ", ") + std::to_string(tenants[i]);
+  // everything the recorded work touches exists before recording starts, and nothing queued on the
+  // handle's stream still reads the pinned tables or the staging slot
+  GS_TRY(gs_reserve_ingest(g, n));
+  GS_CUDA_TRY(cudaStreamSynchronize(s));
+  gs_engine::SliceTables& tb = e->tabs[0];
+  if (n) GS_TRY(stage_slices(tb, slice_tenants, slice_offsets, num_slices));
+  g->labels_valid = false;
+  const bool graph = (flags & GS_PHASE_CUDA_GRAPH) != 0;
+  if (graph) {
+    GS_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    g->capturing = true;
   }
-  if (ierr) {
-    GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, sizeof(uint32_t), s));
-    GS_CUDA_TRY(cudaStreamSynchronize(s));
-    if (ierr & GS_DEV_ERR_VERTEX_RANGE) {
-      gs_set_error("an edge record named a vertex id >= its tenant's num_vertices; those records were skipped");
-      return GS_ERR_BAD_ARG;
+  gs_status st = GS_OK;
+  if (n) {
+    st = copy_slices(tb, num_slices, s);
+    if (st == GS_OK) st = globalize(e, pairs + 2 * first, g->d_pairs, first, n, num_slices, tb, s);
+    if (st == GS_OK) st = gs_ingest_device_pairs(g, g->d_pairs, n, -1, s);
+  }
+  if (st == GS_OK && query_count) st = enqueue_query(e, qp, query_tenants, query_count, s);
+  if (graph) {
+    g->capturing = false;
+    cudaGraph_t cg = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &cg);
+    if (st == GS_OK && ce != cudaSuccess) {
+      gs_set_error(std::string("gs_engine_phase: stream capture failed: ") + cudaGetErrorString(ce));
+      st = GS_ERR_CUDA;
     }
-    gs_set_error("device consistency check failed (bits " + std::to_string(ierr) + ")");
-    return GS_ERR_INTERNAL;
+    if (st == GS_OK) {
+      // same node sequence as the last phase: update the instantiated graph's parameters in place
+      bool updated = false;
+      if (e->phase_exec) {
+        cudaGraphExecUpdateResultInfo info{};
+        updated = cudaGraphExecUpdate(e->phase_exec, cg, &info) == cudaSuccess;
+        if (!updated) {
+          cudaGetLastError();
+          cudaGraphExecDestroy(e->phase_exec);
+          e->phase_exec = nullptr;
+        }
+      }
+      if (!updated) {
+        const cudaError_t ie = cudaGraphInstantiate(&e->phase_exec, cg, 0);
+        if (ie != cudaSuccess) {
+          e->phase_exec = nullptr;
+          gs_set_error(std::string("gs_engine_phase: graph instantiation failed: ") + cudaGetErrorString(ie));
+          st = GS_ERR_CUDA;
+        } else {
+          e->phase_graphs_built++;
+        }
+      }
+      if (st == GS_OK) {
+        const cudaError_t le = cudaGraphLaunch(e->phase_exec, s);
+        if (le != cudaSuccess) {
+          gs_set_error(std::string("gs_engine_phase: graph launch failed: ") + cudaGetErrorString(le));
+          st = GS_ERR_CUDA;
+        } else {
+          e->phase_graph_launches++;
+        }
+      }
+    }
+    if (cg) cudaGraphDestroy(cg);
   }
-  if (!oos.empty()) {
-    gs_set_error("sketches ran out of samples for tenant(s) " + oos);
-    return GS_ERR_SKETCH_FAIL;
-  }
+  GS_TRY(st);
+  GS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (query_count) return finish_query(e, qp, query_tenants, query_count, nullptr, num_cc, rounds);
+  return gs_engine_synchronize(e);
+}
+
+gs_status gs_engine_graph_stats(const gs_engine* e, uint64_t* graphs_built, uint64_t* graph_launches) {
+  if (!e) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  if (graphs_built) *graphs_built = e->phase_graphs_built;
+  if (graph_launches) *graph_launches = e->phase_graph_launches;
   return GS_OK;
 }
 

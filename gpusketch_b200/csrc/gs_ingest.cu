@@ -690,6 +690,12 @@ static gs_status ensure_partition_scratch(gs_graph* g, uint64_t records) {
   return GS_OK;
 }
 
+gs_status gs_reserve_ingest(gs_graph* g, uint64_t edges) {
+  const uint64_t m = std::min<uint64_t>(edges, g->max_batch_edges);
+  GS_TRY(gs_ensure_ingest_scratch(g, std::max<uint64_t>(2 * m, 1)));
+  return ensure_partition_scratch(g, std::max<uint64_t>(2 * m, 1));
+}
+
 static gs_status scan_counts(gs_graph* g, uint32_t nv, cudaStream_t s) {
   const uint32_t tiles = (nv + kScanTile - 1) / kScanTile;
   k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(g->d_cnt, nv, g->tune.chunk, g->d_off, g->d_choff, g->d_tile);

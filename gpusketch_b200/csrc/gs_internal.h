@@ -89,6 +89,7 @@ struct gs_graph {
 
   // ---- profiling ----
   bool prof_on = false;
+  bool capturing = false;                // launches are being recorded into a CUDA graph: no event timing
   std::vector<cudaEvent_t> prof_ev[3];   // [class] begin/end pairs: 0 ingest, 1 bucketing, 2 query
   size_t prof_used[3] = {0, 0, 0};
   uint64_t prof_launches[3] = {0, 0, 0};
@@ -128,6 +129,9 @@ struct GsProfScope {
 // Partial-support helpers implemented in the .cu files.
 gs_status gs_ensure_ingest_scratch(gs_graph* g, uint64_t records);
 gs_status gs_ensure_pair_staging(gs_graph* g);
+// Sizes the single-level ingest scratch for batches of `edges` records, so that a later ingest of
+// at most that many records allocates nothing (required while a stream is being captured).
+gs_status gs_reserve_ingest(gs_graph* g, uint64_t edges);
 
 // Ingest n edge records already on the device (interleaved pairs).  fixed_level < 0: every level
 // the edge tags into (min-cut) or level 0 (connected components); >= 0: that level only.

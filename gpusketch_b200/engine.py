@@ -13,7 +13,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import GS_ERR_OOM, GpuSketchError, GsEngineConfig, GsGeometry, GsProfile, check, lib
+from ._native import GS_ERR_OOM, GS_PHASE_CUDA_GRAPH, GpuSketchError, GsEngineConfig, GsGeometry, GsProfile, check, lib
 from .graph import BUCKET_DTYPE, Geometry, _as_pairs, _stream_ptr
 
 
@@ -87,6 +87,10 @@ class SketchEngine:
         check(self._lib.gs_engine_remove_tenant(self._h, tenant), "gs_engine_remove_tenant")
         self.tenants.pop(tenant, None)
 
+    def clear_tenant(self, tenant: int) -> None:
+        """Zero one tenant's sketches."""
+        check(self._lib.gs_engine_clear_tenant(self._h, tenant), "gs_engine_clear_tenant")
+
     def memory(self) -> tuple[int, int, int]:
         """(sketch bytes in use, arena bytes, live tenants)."""
         u, c, n = C.c_uint64(), C.c_uint64(), C.c_uint32()
@@ -122,8 +126,54 @@ class SketchEngine:
             return
         self.ingest(tens, offs, np.concatenate(parts) if len(parts) > 1 else parts[0], stream)
 
+    def ingest_slices(self, batches, stream=None) -> None:
+        """batches: iterable of (tenant, (n, 2) uint32 host array or CPU tensor), one coalesced ingest
+        without concatenating on the host (page-locked arrays are copied to the device directly)."""
+        keep, tens, counts, ptrs = [], [], [], []
+        for t, a in batches:
+            p, n, dev, k = _as_pairs(a)
+            if dev:
+                raise ValueError("ingest_slices takes host records")
+            keep.append(k)
+            tens.append(t)
+            counts.append(n)
+            ptrs.append(p.value or 0)
+        if not tens:
+            return
+        st = np.array(tens, np.uint32)
+        sc = np.array(counts, np.uint64)
+        sp = (C.c_void_p * len(ptrs))(*ptrs)
+        check(self._lib.gs_engine_ingest_slices(self._h, len(tens), st.ctypes.data, sc.ctypes.data, sp,
+                                                _stream_ptr(stream)), "gs_engine_ingest_slices")
+        del keep
+
     def synchronize(self) -> None:
         check(self._lib.gs_engine_synchronize(self._h), "gs_engine_synchronize")
+
+    def phase(self, slice_tenants, slice_offsets, pairs, query_tenants=(), cuda_graph: bool = True) -> dict:
+        """One batched phase: ingest device-resident slices, then query `query_tenants` (no labels).
+        With cuda_graph the phase's device work runs as one CUDA graph.  {tenant: (num_cc, rounds)}."""
+        st = np.ascontiguousarray(slice_tenants, dtype=np.uint32)
+        so = np.ascontiguousarray(slice_offsets, dtype=np.uint64)
+        if so.size != st.size + 1:
+            raise ValueError("slice_offsets needs one entry more than slice_tenants")
+        p, _, dev, keep = _as_pairs(pairs)
+        if not dev and st.size:
+            raise ValueError("phase() takes device-resident records (a CUDA tensor)")
+        qt = np.ascontiguousarray(list(query_tenants), dtype=np.uint32)
+        ncc = np.zeros(max(qt.size, 1), np.uint32)
+        rounds = np.zeros(max(qt.size, 1), np.uint32)
+        check(self._lib.gs_engine_phase(self._h, st.ctypes.data, so.ctypes.data, st.size, p, qt.ctypes.data, qt.size,
+                                        ncc.ctypes.data, rounds.ctypes.data,
+                                        GS_PHASE_CUDA_GRAPH if cuda_graph else 0), "gs_engine_phase")
+        del keep
+        return {int(t): (int(ncc[i]), int(rounds[i])) for i, t in enumerate(qt)}
+
+    def graph_stats(self) -> tuple[int, int]:
+        """(CUDA graphs instantiated, CUDA graph launches) by phase() so far."""
+        b, l = C.c_uint64(), C.c_uint64()
+        check(self._lib.gs_engine_graph_stats(self._h, C.byref(b), C.byref(l)), "gs_engine_graph_stats")
+        return b.value, l.value
 
     # ---- queries ----
     def connected_components(self, tenants, with_labels: bool = True) -> dict[int, TenantResult]:

@@ -270,6 +270,8 @@ gs_status gs_engine_tenant_bytes(uint32_t num_vertices, double sketches_factor, 
 gs_status gs_engine_add_tenant(gs_engine* e, uint32_t num_vertices, uint64_t seed, double sketches_factor,
                                uint32_t* tenant);
 gs_status gs_engine_remove_tenant(gs_engine* e, uint32_t tenant);
+/* Zeroes one tenant's sketches (Sketch::zero_contents over its vertices, src/sketch.cpp:102-108). */
+gs_status gs_engine_clear_tenant(gs_engine* e, uint32_t tenant);
 /* Sketch bytes in use by live tenants, the arena size, and the live tenant count. */
 gs_status gs_engine_memory(const gs_engine* e, uint64_t* used, uint64_t* capacity, uint32_t* live_tenants);
 gs_status gs_engine_set_stream(gs_engine* e, void* cuda_stream);
@@ -281,6 +283,14 @@ gs_status gs_engine_set_stream(gs_engine* e, void* cuda_stream);
  * gs_engine_synchronize or query. */
 gs_status gs_engine_ingest(gs_engine* e, const uint32_t* slice_tenants, const uint64_t* slice_offsets,
                            uint32_t num_slices, const uint32_t* pairs, int pairs_on_device, void* cuda_stream);
+/* Gather form for serving: slice i is slice_counts[i] records at HOST address slice_pairs[i] for
+ * tenant slice_tenants[i]; the slices are coalesced into one bucketing pass and one sketch update.
+ * Page-locked slices are copied to the device directly, others through the pinned staging ring.
+ * Returns once the caller's buffers may be reused; the device work may still be running (the copy
+ * of the next call overlaps it). */
+gs_status gs_engine_ingest_slices(gs_engine* e, uint32_t num_slices, const uint32_t* slice_tenants,
+                                  const uint64_t* slice_counts, const uint32_t* const* slice_pairs,
+                                  void* cuda_stream);
 gs_status gs_engine_synchronize(gs_engine* e);
 /* connected_components() of `count` distinct tenants in one device Boruvka launch.  labels
  * (host, may be NULL) receives each listed tenant's V labels back to back in list order, each the
@@ -289,6 +299,20 @@ gs_status gs_engine_synchronize(gs_engine* e);
  * out of samples (OutOfSamplesException); the others' results are still written. */
 gs_status gs_engine_connected_components(gs_engine* e, const uint32_t* tenants, uint32_t count, uint32_t* labels,
                                          uint32_t* num_cc, uint32_t* rounds);
+/* One phase of a batched workload: ingest slices of DEVICE-resident records (as gs_engine_ingest,
+ * at most 2^25 records) and then answer connected_components() for `query_count` tenants (as
+ * gs_engine_connected_components without labels; query_count may be 0).  With
+ * GS_PHASE_CUDA_GRAPH in `flags` the phase's device work - slice-table upload, endpoint bucketing,
+ * sketch update, the persistent Boruvka kernel and the result read-back - is recorded into one CUDA
+ * graph and launched as a whole; a phase with the same sequence of steps as the previous one
+ * updates that graph's parameters in place instead of instantiating a new one.  Returns after
+ * the phase finished. */
+#define GS_PHASE_CUDA_GRAPH 1
+gs_status gs_engine_phase(gs_engine* e, const uint32_t* slice_tenants, const uint64_t* slice_offsets,
+                          uint32_t num_slices, const uint32_t* pairs, const uint32_t* query_tenants,
+                          uint32_t query_count, uint32_t* num_cc, uint32_t* rounds, int flags);
+/* CUDA graphs instantiated and launched by gs_engine_phase so far. */
+gs_status gs_engine_graph_stats(const gs_engine* e, uint64_t* graphs_built, uint64_t* graph_launches);
 gs_status gs_engine_tenant_geometry(const gs_engine* e, uint32_t tenant, gs_geometry* out);
 /* Tenant sketches of vertices [first, first+count) to host memory, in the write_binary layout. */
 gs_status gs_engine_download_sketches(gs_engine* e, uint32_t tenant, uint32_t first, uint32_t count,

@@ -49,7 +49,7 @@ def solo(V, seed, factor, pairs):
 
 
 def make_engine(budget_mb=256, max_tenants=16, max_vertices=1 << 16, max_tenant_vertices=1 << 14):
-    return SketchEngine(budget_mb << 20, max_tenants, max_vertices, max_tenant_vertices)
+    return SketchEngine(budget_mb << 20, max_tenants, max_vertices, max_tenant_vertices, max_batch_edges=1 << 20)
 
 
 @pytest.mark.parametrize("device_input", [False, True])
@@ -129,7 +129,7 @@ def test_phases_and_incremental_ingest(restatement):
 def test_admission_by_sketch_bytes_and_slot_reuse():
     per = tenant_bytes(4096)
     budget = 3 * per + per // 2
-    with SketchEngine(budget, 8, 1 << 15, 4096) as e:
+    with SketchEngine(budget, 8, 1 << 15, 4096, max_batch_edges=1 << 20) as e:
         ids = [e.add_tenant(4096, 100 + i) for i in range(3)]
         used, cap, live = e.memory()
         assert (used, live) == (3 * per, 3) and cap >= budget - 16
@@ -154,7 +154,7 @@ def test_admission_by_sketch_bytes_and_slot_reuse():
 
 
 def test_tenant_slots_and_vertex_space_limits():
-    with SketchEngine(64 << 20, 2, 3000, 2048) as e:
+    with SketchEngine(64 << 20, 2, 3000, 2048, max_batch_edges=1 << 20) as e:
         a = e.add_tenant(2048, 1)
         assert e.try_add_tenant(1024, 2) is None               # vertex space: 2048 + 1024 > 3000
         b = e.add_tenant(900, 3)
@@ -200,3 +200,90 @@ def test_write_binary_per_tenant_reloads(tmp_path):
         assert open(path, "rb").read() == open(ref, "rb").read()
         with gs.GraphSketch.read_binary(path) as back:
             assert back.connected_components()[1] == e.connected_components([t])[t].num_cc
+
+
+def test_phase_cuda_graph_matches_eager_and_exact(restatement):
+    """Batched phases (device records, one query per phase) with and without CUDA-graph capture."""
+    import torch
+    from gpusketch_b200.workloads import batched_streams, phase_slices
+    streams = batched_streams(12)
+    phases = 3
+    slices = phase_slices(streams, phases)
+    results = []
+    for graph in (True, False):
+        with SketchEngine(1 << 30, 16, sum(s.V for s in streams), 1 << 14, max_batch_edges=1 << 20) as e:
+            ids = [e.add_tenant(s.V, s.sketch_seed) for s in streams]
+            per_phase = []
+            for p in range(phases):
+                parts = [s.records[lo:hi] for s, (lo, hi) in zip(streams, slices[p])]
+                offs = np.cumsum([0] + [len(x) for x in parts]).astype(np.uint64)
+                d = torch.from_numpy(np.concatenate(parts).astype(np.int32)).cuda()
+                per_phase.append(e.phase(ids, offs, d, ids, cuda_graph=graph))
+            if graph:
+                built, launched = e.graph_stats()
+                assert launched == phases and 1 <= built <= phases
+            results.append((per_phase, [e.download(t).tobytes() for t in ids]))
+    assert results[0] == results[1]
+    per_phase, sk = results[0]
+    for k, s in enumerate(streams):
+        hi = slices[phases - 1][k][1]
+        _, exact = restatement.exact_cc(s.V, s.records[:hi])
+        assert per_phase[-1][k][0] == len(np.unique(exact)), k
+        _, exact1 = restatement.exact_cc(s.V, s.records[:slices[0][k][1]])
+        assert per_phase[0][k][0] == len(np.unique(exact1)), k
+        sk_solo, *_ = solo(s.V, s.sketch_seed, 1.0, s.records)
+        assert sk[k] == sk_solo, k
+
+
+def test_ingest_slices_pinned_and_pageable():
+    import torch
+    with make_engine() as e:
+        specs = TENANTS[:3]
+        ids = [e.add_tenant(V, seed, f) for V, seed, f, _ in specs]
+        streams = [gen() for *_, gen in specs]
+        batches = []
+        for k, (t, a) in enumerate(zip(ids, streams)):
+            half = len(a) // 2
+            pinned = torch.from_numpy(a[:half].astype(np.int32)).pin_memory()
+            batches += [(t, pinned), (t, a[half:])]
+        e.ingest_slices(batches[::-1])
+        e.ingest_slices([])
+        for (V, seed, f, _), t, a in zip(specs, ids, streams):
+            sk, *_ = solo(V, seed, f, a)
+            assert e.download(t).tobytes() == sk
+
+
+def test_served_answers_match_solo_runs():
+    """Continuous batching with admission: each answer equals the tenant's solo prefix, exactly."""
+    from gpusketch_b200.serve import SketchServer
+    from gpusketch_b200.workloads import served_trace
+    tr = served_trace(num_tenants=8, duration_s=0.25, mean_gap_ms=2.0, query_frac=0.3, log2_batch=(6.0, 11.0),
+                      seed=77)
+    for i, (V, lg, seed) in enumerate(tr.tenants):       # keep the solo checks small
+        v = 1 << (10 + i % 3)
+        tr.tenants[i] = (v, 10 + i % 3, seed)
+    budget = sum(sorted(tenant_bytes(v) for v, _, _ in tr.tenants)[-3:]) + 4096
+    srv = SketchServer(tr, budget, keep_labels=True, keep_sketches=True)
+    try:
+        stats = srv.run(srv.prepare())
+    finally:
+        srv.close()
+    assert stats.max_live_tenants < len(tr.tenants)     # admission by sketch bytes kept some waiting
+    assert stats.answers and stats.updates > 0
+    for a in stats.answers:
+        V, _, seed = tr.tenants[a.tenant]
+        with gs.GraphSketch(V, seed) as g:
+            if a.records_before:
+                g.ingest_pairs(tr.tenant_records(a.tenant, 0, a.records_before))
+            labels, ncc, _ = g.connected_components()
+        assert a.num_cc == ncc and np.array_equal(a.labels, labels), a.request
+    total = {}
+    for r in tr.requests:
+        if r.kind == "update":
+            total[r.tenant] = total.get(r.tenant, 0) + r.n
+    for t, sk in stats.final_sketches.items():
+        V, _, seed = tr.tenants[t]
+        with gs.GraphSketch(V, seed) as g:
+            if total.get(t):
+                g.ingest_pairs(tr.tenant_records(t, 0, total[t]))
+            assert g.download().tobytes() == sk, t
