@@ -27,6 +27,9 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from gpusketch_b200.replicas import (barrier as rank_barrier, env_rank, max_over_ranks as rank_max,
+                                     replica_seed, sum_over_ranks, whole_job_rate)
+
 V_LOG2 = 17
 STREAM_SEED = 0x5EED0002
 SKETCH_SEED = 0xC0FFEE
@@ -52,11 +55,6 @@ def parse_args():
     ap.add_argument("--batched-phases", type=int, default=4)
     ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request trace")
     return ap.parse_args()
-
-
-def env_rank():
-    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
-            int(os.environ.get("LOCAL_RANK", 0)))
 
 
 def measured_peak_hbm():
@@ -295,7 +293,7 @@ def run_batched(args, dev, steps, warmup):
         h.close()
     agree = all(plain_res[p][t] == eng_res[p][t][0] == eager_res[p][t][0] for p in range(P) for t in ids)
     return {
-        "workload": f"batched_{len(streams)}_er_streams", "streams": len(streams), "phases": P,
+        "workload": f"batched_{len(streams)}_er_streams", "scope": "one GPU (rank 0)", "streams": len(streams), "phases": P,
         "updates_per_step": total, "vertices": sum(s.V for s in streams), "sketch_bytes": used,
         "engine_value": total / eng_s, "engine_eager_value": total / eager_s, "plain_value": total / plain_s,
         "unit": UNIT, "speedup_vs_plain": plain_s / eng_s, "engine_ms_per_step": 1e3 * eng_s,
@@ -330,7 +328,7 @@ def run_served(args, dev):
 
     offered = sum(r.n for r in tr.requests if r.kind == "update")
     return {
-        "workload": "served_64_tenants_rmat", "tenants": len(tr.tenants), "requests": len(tr.requests),
+        "workload": "served_64_tenants_rmat", "scope": "one GPU (rank 0)", "tenants": len(tr.tenants), "requests": len(tr.requests),
         "queries": len(st.answers), "trace_seconds": args.served_seconds, "offered_updates": offered,
         "query_latency_ms": st.latency_summary(), "updates_per_s": st.updates_per_s,
         "plain_query_latency_ms": pst.latency_summary(), "plain_updates_per_s": pst.updates_per_s,
@@ -357,14 +355,14 @@ def run_gs(args):
     U = 1 << args.updates_log2
     phase = 1 << args.phase_log2
     P = U // phase
-    stream_seed = STREAM_SEED + rank
+    stream_seed = replica_seed(STREAM_SEED, rank)
     dev = torch.device("cuda", local)
 
     d_in = torch.empty((U, 2), dtype=torch.int32, device=dev)
     gs.rmat_stream(V_LOG2, U, stream_seed, out=d_in)
     torch.cuda.synchronize()
 
-    g = gs.GraphSketch(V, SKETCH_SEED + rank, device=local, max_batch_edges=phase)
+    g = gs.GraphSketch(V, replica_seed(SKETCH_SEED, rank), device=local, max_batch_edges=phase)
     ts = torch.cuda.current_stream()
     g.set_stream(ts)
     geo = g.geometry
@@ -385,15 +383,10 @@ def run_gs(args):
             g.connected_components()
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        rank_barrier(dist)
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, dist, dev)
 
     for _ in range(args.warmup):
         step(d_in)
@@ -414,7 +407,7 @@ def run_gs(args):
     clocks = clk.summary()
     ms_max = max_over_ranks(ms)
     ms_per_step = ms_max / args.steps
-    value = world * U * args.steps / (ms_max / 1e3)
+    value = whole_job_rate(sum_over_ranks(U * args.steps, dist, dev), ms_max)
 
     # roofline of the dominant kernel (the sketch update), per launch: B_edge = 8 + 2*V*S_v/U_phase
     # bytes per edge update (the read half dropped for the first phase of a step, whose sketches are 0)
@@ -454,7 +447,7 @@ def run_gs(args):
         torch.cuda.synchronize()
         barrier()
         ems = max_over_ranks(e_start.elapsed_time(e_end))
-        e2e = {"value": world * U * args.steps / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": U * 8,
+        e2e = {"value": whole_job_rate(world * U * args.steps, ems), "unit": UNIT, "h2d_bytes_per_step": U * 8,
                "d2h_bytes_per_step": P * V * 4, "ms_per_step": ems / args.steps}
         del h_in
 
