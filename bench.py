@@ -51,6 +51,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target wall time of the CPU sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-stream batched engine comparison")
     ap.add_argument("--no-served", action="store_true", help="skip the 64-tenant served trace")
+    ap.add_argument("--no-mincut", action="store_true", help="skip the planted-cut min-cut workload")
     ap.add_argument("--batched-streams", type=int, default=256)
     ap.add_argument("--batched-phases", type=int, default=4)
     ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request trace")
@@ -339,6 +340,39 @@ def run_served(args, dev):
     }
 
 
+def run_mincut(args, dev):
+    """k-connectivity / min cut: V=2^14 as two ER blocks of 8192 (p=0.3) joined by 3 planted edges,
+    inserted in random order then 5% deleted and re-inserted (~22M records); k=4 forests per level over
+    4 sketched subgraph levels (tags get_index_depth(e, seed, L-1), L = 1 + 2 log2 V).  Timed: the
+    tagged ingest of the device-resident records, then the level-by-level min-cut driver."""
+    import numpy as np
+    import torch
+    import gpusketch_b200 as gs
+    from gpusketch_b200.workloads import planted_cut_stream
+    n = 8192
+    recs, _ = planted_cut_stream(n)
+    V = 2 * n
+    L = 1 + 2 * int(np.log2(V))
+    d = torch.from_numpy(recs.astype(np.int32)).to(dev)
+    g = gs.GraphSketch(V, 0x5EED0003, num_levels=4, num_subgraphs=L, device=dev.index, max_batch_edges=1 << 25)
+    g.ingest_pairs(d)            # warm-up of the same work, then cleared
+    g.min_cut(4)
+    g.clear()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.ingest_pairs(d)
+    g.synchronize()
+    t1 = time.perf_counter()
+    value, level, cut_at, side = g.min_cut(4)
+    t2 = time.perf_counter()
+    g.close()
+    return {"workload": "mincut_planted_v16384", "scope": "one GPU (rank 0)", "records": int(len(recs)),
+            "levels": 4, "k": 4, "num_subgraphs": L, "ingest_updates_per_s": len(recs) / (t1 - t0),
+            "ingest_ms": 1e3 * (t1 - t0), "min_cut_ms": 1e3 * (t2 - t1), "value": value, "expected": 3,
+            "level": level, "cut_at_level": cut_at,
+            "timing": "wall clock around synchronous calls, device idle on both sides"}
+
+
 def run_gs(args):
     import numpy as np
     import torch
@@ -462,7 +496,9 @@ def run_gs(args):
     g.close()
     del d_in
     torch.cuda.empty_cache()
-    batched = served = None
+    batched = served = mincut = None
+    if not args.no_mincut:
+        mincut = run_mincut(args, dev)
     if not args.no_batched:
         batched = run_batched(args, dev, max(1, args.steps), max(1, args.warmup))
     if not args.no_served:
@@ -482,6 +518,7 @@ def run_gs(args):
                    "parallelism": f"replicas x{world}", "tuning": tuning},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": prof["kernel_launches"],
         "clocks": clocks, "kernel_split": split, "batched": batched, "served": served,
+        "mincut": mincut,
     }
     if os.environ.get("GS_BENCH_TUNE_TABLE"):
         line["tune_table"] = tune_table

@@ -100,3 +100,19 @@ def served_trace(num_tenants: int = 64, duration_s: float = 1.0, mean_gap_ms: fl
             tr.requests.append(Request(t, k, "update", cursor[k], n))
             cursor[k] += n
     return tr
+
+
+def planted_cut_stream(n_block: int = 8192, p: float = 0.3, cut: int = 3, churn: float = 0.05,
+                       seed: int = 0x5EED0003) -> tuple[np.ndarray, np.ndarray]:
+    """Two Erdos-Renyi blocks G(n_block, p) on [0, n) and [n, 2n) joined by `cut` random cross edges,
+    inserted in random order, then a `churn` share of the edges deleted and re-inserted.
+    Returns (records, the planted cut edges)."""
+    rng = np.random.default_rng(seed)
+    a = er_stream(n_block, p, seed)
+    b = er_stream(n_block, p, seed + 1) + np.uint32(n_block)
+    cross = np.stack([rng.integers(0, n_block, cut), rng.integers(n_block, 2 * n_block, cut)], 1).astype(np.uint32)
+    edges = np.concatenate([a, b, cross])
+    edges = edges[rng.permutation(len(edges))]
+    k = int(churn * len(edges))
+    pick = edges[rng.choice(len(edges), size=k, replace=False)]
+    return np.concatenate([edges, pick, pick]), cross

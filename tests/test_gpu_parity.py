@@ -324,3 +324,19 @@ def test_autotune_keeps_sketches(torch_cuda):
         best = autotune(g, d, chunks=(512, 4096), warps=(4, 8), reg_depths=(1, 2))
         assert sketch_bytes(g) == before
         assert best["reg_depth"] in (1, 2)
+
+
+def test_min_cut_full_config():
+    """V=2^14: two ER blocks of 8192 (p=0.3, ~20M edges) joined by 3 planted edges, 5% delete and
+    re-insert, k=4 forests per level: the min cut is the planted 3 and its side is one block."""
+    from gpusketch_b200.workloads import planted_cut_stream
+    n = 8192
+    recs, cross = planted_cut_stream(n)
+    V = 2 * n
+    L = 1 + 2 * int(np.log2(V))
+    alg = gs.MCGPUSketchAlg(V, 0x5EED0003, num_subgraphs=L, max_sketch_graphs=4, k=4)
+    alg.ingest_pairs(recs)
+    value, level, cut_at, side = alg.sketches().min_cut(4)
+    assert (value, level, cut_at) == (3, 0, 3)
+    s = side.astype(bool)
+    assert s[:n].all() != s[n:].all() and (s[:n].all() or not s[:n].any()) and (s[n:].all() or not s[n:].any())
