@@ -211,6 +211,84 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter(const uint2* __re
   }
 }
 
+// Pass 1 placement when every edge makes exactly two records (one level): each thread keeps its
+// edges' bucket ranks in registers, the block's records are sorted by bucket in shared memory, and
+// each bucket's run is written out with consecutive threads on consecutive addresses.  The edges
+// are read once (the generic kernel above reads them twice and scatters 8-byte writes).
+constexpr int kStageEdgesPerThread = kPartEdges / kPartThreads;
+
+size_t part_scatter_staged_smem(uint32_t H) {
+  return (size_t)((3 * H + 1 + 1) & ~1u) * sizeof(uint32_t) + (size_t)2 * kPartEdges * sizeof(uint2);
+}
+
+__global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint2* __restrict__ pairs, uint64_t n,
+                                                                      PairTag t, uint32_t lb, uint32_t H,
+                                                                      uint32_t* __restrict__ bkt,
+                                                                      uint2* __restrict__ part, uint64_t cap,
+                                                                      uint32_t* __restrict__ status) {
+  extern __shared__ uint32_t sh[];
+  uint32_t* hist = sh;            // [H] records per bucket, then ranks
+  uint32_t* loff = sh + H;        // [H] exclusive offsets in the block's sorted order
+  uint32_t* gbase = sh + 2 * H;   // [H] first global position of the block's run of each bucket
+  uint32_t* s_total = sh + 3 * H;
+  uint2* stage = reinterpret_cast<uint2*>(sh + ((3 * H + 1 + 1) & ~1u));  // [2 * kPartEdges]
+  uint32_t* cur = bkt + 2 * H + 1;
+  const uint32_t lvl = t.fixed_level >= 0 ? (uint32_t)t.fixed_level : 0u;
+  for (uint32_t i = threadIdx.x; i < H; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const uint64_t e0 = (uint64_t)blockIdx.x * kPartEdges;
+  uint32_t ku[kStageEdgesPerThread], kv[kStageEdgesPerThread], ru[kStageEdgesPerThread], rv[kStageEdgesPerThread];
+#pragma unroll
+  for (int k = 0; k < kStageEdgesPerThread; k++) {
+    const uint64_t e = e0 + threadIdx.x + (uint64_t)k * kPartThreads;
+    ku[k] = 0xffffffffu;
+    if (e < n) {
+      const uint2 p = pairs[e];
+      if (p.x < t.V && p.y < t.V && p.x != p.y) {  // out-of-range records were reported by k_part_count
+        ku[k] = lvl * t.V + p.x;
+        kv[k] = lvl * t.V + p.y;
+        ru[k] = atomicAdd(&hist[ku[k] >> lb], 1u);
+        rv[k] = atomicAdd(&hist[kv[k] >> lb], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  // exclusive scan of the block histogram: thread i owns buckets [i*per, (i+1)*per)
+  {
+    const uint32_t per = (H + blockDim.x - 1) / blockDim.x;
+    const uint32_t b0 = min(H, threadIdx.x * per), b1 = min(H, b0 + per);
+    uint32_t sum = 0;
+    for (uint32_t b = b0; b < b1; b++) sum += hist[b];
+    uint2 tot;
+    const uint2 ex = block_exclusive_scan(make_uint2(sum, 0u), &tot);
+    uint32_t run = ex.x;
+    for (uint32_t b = b0; b < b1; b++) {
+      const uint32_t c = hist[b];
+      loff[b] = run;
+      gbase[b] = c ? atomicAdd(&cur[b], c) : 0u;
+      run += c;
+    }
+    if (threadIdx.x == 0) *s_total = tot.x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kStageEdgesPerThread; k++) {
+    if (ku[k] == 0xffffffffu) continue;
+    const uint32_t nu = kv[k] - lvl * t.V, nv = ku[k] - lvl * t.V;
+    stage[loff[ku[k] >> lb] + ru[k]] = make_uint2(ku[k], nu);
+    stage[loff[kv[k] >> lb] + rv[k]] = make_uint2(kv[k], nv);
+  }
+  __syncthreads();
+  const uint32_t total = *s_total;
+  for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+    const uint2 r = stage[i];
+    const uint32_t b = r.x >> lb;
+    const uint64_t pos = (uint64_t)gbase[b] + (i - loff[b]);
+    if (pos < cap) part[pos] = r;
+    else atomicOr(status, (uint32_t)GS_DEV_ERR_CAPACITY);
+  }
+}
+
 // the bucket of pass-2 chunk c: largest d with choff[d] <= c
 __device__ __forceinline__ uint32_t chunk_bucket(const uint32_t* choff, uint32_t H, uint32_t c) {
   uint32_t lo = 0, hi = H;
@@ -278,6 +356,83 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __re
       const uint2 r = part[i];
       const uint32_t k = r.x & mask;
       const uint32_t pos = base[k] + atomicAdd(&hist[k], 1u);
+      if (pos < cap) nbr[pos] = r.y;
+      else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
+    }
+    __syncthreads();
+  }
+}
+
+// Pass 2 placement with the chunk's records sorted by vertex in shared memory first, so that every
+// vertex's run of neighbours is written by consecutive threads to consecutive addresses.
+constexpr int kVertPerThread = kVertChunk / kPartThreads;
+constexpr size_t kStagedSmemLimit = 200 * 1024;
+
+size_t vert_scatter_staged_smem(uint32_t lb) {
+  const uint32_t nk = 1u << lb;
+  return (size_t)((3 * nk + 2 + 1) & ~1u) * sizeof(uint32_t) + (size_t)kVertChunk * sizeof(uint2);
+}
+
+__global__ void __launch_bounds__(kPartThreads, 2) k_vert_scatter_staged(const uint2* __restrict__ part,
+                                                                      const uint32_t* __restrict__ bkt, uint32_t H,
+                                                                      uint32_t lb, uint32_t* __restrict__ cursor,
+                                                                      uint32_t* __restrict__ nbr, uint64_t cap,
+                                                                      uint32_t* __restrict__ status) {
+  extern __shared__ uint32_t sh[];
+  const uint32_t nk = 1u << lb, mask = nk - 1;
+  uint32_t* hist = sh;          // [nk]
+  uint32_t* loff = sh + nk;     // [nk]
+  uint32_t* gbase = sh + 2 * nk;
+  uint32_t* s_d = sh + 3 * nk;  // [2]: bucket of the chunk, records in it
+  uint2* stage = reinterpret_cast<uint2*>(sh + ((3 * nk + 2 + 1) & ~1u));
+  const uint32_t* off = bkt + H;
+  const uint32_t* choff = bkt + 3 * H + 1;
+  const uint32_t total = status[5];
+  for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+    if (threadIdx.x == 0) s_d[0] = chunk_bucket(choff, H, c);
+    for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const uint32_t d = s_d[0];
+    const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
+    const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
+    uint32_t key[kVertPerThread], nb[kVertPerThread], rk[kVertPerThread];
+#pragma unroll
+    for (int k = 0; k < kVertPerThread; k++) {
+      const uint32_t i = r0 + threadIdx.x + (uint32_t)k * kPartThreads;
+      key[k] = 0xffffffffu;
+      if (i < r1) {
+        const uint2 r = part[i];
+        key[k] = r.x & mask;
+        nb[k] = r.y;
+        rk[k] = atomicAdd(&hist[key[k]], 1u);
+      }
+    }
+    __syncthreads();
+    {
+      const uint32_t per = (nk + blockDim.x - 1) / blockDim.x;
+      const uint32_t b0 = min(nk, threadIdx.x * per), b1 = min(nk, b0 + per);
+      uint32_t sum = 0;
+      for (uint32_t b = b0; b < b1; b++) sum += hist[b];
+      uint2 tot;
+      const uint2 ex = block_exclusive_scan(make_uint2(sum, 0u), &tot);
+      uint32_t run = ex.x;
+      for (uint32_t b = b0; b < b1; b++) {
+        const uint32_t h = hist[b];
+        loff[b] = run;
+        gbase[b] = h ? atomicAdd(&cursor[(d << lb) + b], h) : 0u;
+        run += h;
+      }
+      if (threadIdx.x == 0) s_d[1] = tot.x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kVertPerThread; k++)
+      if (key[k] != 0xffffffffu) stage[loff[key[k]] + rk[k]] = make_uint2(key[k], nb[k]);
+    __syncthreads();
+    const uint32_t n = s_d[1];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint2 r = stage[i];
+      const uint64_t pos = (uint64_t)gbase[r.x] + (i - loff[r.x]);
       if (pos < cap) nbr[pos] = r.y;
       else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
     }
@@ -646,6 +801,37 @@ gs_status launch_ingest_s(gs_graph* g, uint32_t nv, bool small, cudaStream_t s) 
   return small ? launch_ingest_r<CG, true, TEN>(g, nv, s) : launch_ingest_r<CG, false, TEN>(g, nv, s);
 }
 
+gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& t, uint32_t lb, uint32_t H,
+                                     uint32_t* bkt, uint2* part, uint64_t cap, uint32_t* status, cudaStream_t s) {
+  const size_t smem = part_scatter_staged_smem(H);
+  static size_t smem_set[64] = {};
+  int dev = 0;
+  GS_CUDA_TRY(cudaGetDevice(&dev));
+  if (smem_set[dev & 63] < smem) {
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_part_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    smem_set[dev & 63] = smem;
+  }
+  const unsigned tiles = (unsigned)((m + kPartEdges - 1) / kPartEdges);
+  k_part_scatter_staged<<<tiles, kPartThreads, smem, s>>>(p, m, t, lb, H, bkt, part, cap, status);
+  GS_CUDA_TRY(cudaGetLastError());
+  return GS_OK;
+}
+
+gs_status launch_vert_scatter_staged(const uint2* part, const uint32_t* bkt, uint32_t H, uint32_t lb, uint32_t* cursor,
+                                     uint32_t* nbr, uint64_t cap, uint32_t* status, int grid, cudaStream_t s) {
+  const size_t smem = vert_scatter_staged_smem(lb);
+  static size_t smem_set[64] = {};
+  int dev = 0;
+  GS_CUDA_TRY(cudaGetDevice(&dev));
+  if (smem_set[dev & 63] < smem) {
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_vert_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    smem_set[dev & 63] = smem;
+  }
+  k_vert_scatter_staged<<<grid, kPartThreads, smem, s>>>(part, bkt, H, lb, cursor, nbr, cap, status);
+  GS_CUDA_TRY(cudaGetLastError());
+  return GS_OK;
+}
+
 }  // namespace
 
 gs_status gs_ensure_ingest_scratch(gs_graph* g, uint64_t records) {
@@ -757,13 +943,22 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
     }
     {
       GsProfScope ps(g, GS_PROF_BUCKET, s, 6);
-      k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, m, t, lb, H, g->d_bkt, g->d_part,
-                                                                           g->part_cap, g->d_status);
+      if (tagged) {
+        k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, m, t, lb, H, g->d_bkt, g->d_part,
+                                                                             g->part_cap, g->d_status);
+      } else {
+        GS_TRY(launch_part_scatter_staged(p, m, t, lb, H, g->d_bkt, g->d_part, g->part_cap, g->d_status, s));
+      }
       k_vert_count<<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt,
                                                                              g->d_status);
       GS_TRY(scan_counts(g, nv, s));
-      k_vert_scatter<<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(
-          g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status);
+      if (vert_scatter_staged_smem(lb) <= kStagedSmemLimit) {
+        GS_TRY(launch_vert_scatter_staged(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status,
+                                          grid2, s));
+      } else {  // very large vertex spaces: the per-vertex tables of a bucket no longer fit beside the stage
+        k_vert_scatter<<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(
+            g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status);
+      }
       GS_CUDA_TRY(cudaGetLastError());
     }
     {
