@@ -541,8 +541,8 @@ extern "C" gs_status gs_get_tuning(const gs_graph* g, gs_tuning* out) {
 extern "C" gs_status gs_set_tuning(gs_graph* g, const gs_tuning* t) {
   if (!g || !t) { gs_set_error("null argument"); return GS_ERR_BAD_ARG; }
   if (t->chunk < 32 || t->chunk > (1u << 20) || t->warps_per_block < 1 || t->warps_per_block > 16 ||
-      t->reg_depth < 1 || t->reg_depth > 3) {
-    gs_set_error("gs_set_tuning: chunk in [32, 2^20], warps_per_block in [1, 16], reg_depth in [1, 3]");
+      t->reg_depth > 3) {
+    gs_set_error("gs_set_tuning: chunk in [32, 2^20], warps_per_block in [1, 16], reg_depth in [0, 3]");
     return GS_ERR_BAD_ARG;
   }
   g->tune.chunk = t->chunk;

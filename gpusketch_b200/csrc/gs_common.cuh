@@ -103,11 +103,10 @@ __device__ __forceinline__ uint32_t gs_depth_from_mixed(uint64_t x, uint32_t max
   h *= kGsMx2;
   const uint32_t l2 = (uint32_t)h, h2 = (uint32_t)(h >> 32);
   const uint32_t flo = l2 ^ (h2 * 16u) ^ __umulhi(l2, 16u);
-  // ctz of the 64-bit value without a branch: clz(brev(0)) = 32, so the high word only decides when
-  // the low word is zero
-  const uint32_t dlo = __clz(__brev(flo));
-  const uint32_t dhi = 32u + __clz(__brev(h2 ^ (h2 >> 28)));
-  const uint32_t d = flo ? dlo : dhi;
+  // ctz of the 64-bit value: the high word only decides when the low word is zero (probability
+  // 2^-32), so it is computed in a branch that practically never runs
+  uint32_t d = __clz(__brev(flo));
+  if (__builtin_expect(flo == 0u, 0)) d = 32u + __clz(__brev(h2 ^ (h2 >> 28)));
   return d < max_depth ? d : max_depth;
 }
 #endif

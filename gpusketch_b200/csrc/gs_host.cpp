@@ -55,8 +55,8 @@ GsTuning gs_tune_for(const GsGeom& geom, int num_sms) {
   (void)num_sms;
   GsTuning t;
   t.chunk = 256;           // defaults measured best on B200 for the V=2^17 R-MAT stream; the
-  t.warps_per_block = 8;   // autotuner refines them per geometry
-  t.reg_depth = 1;
+  t.warps_per_block = 16;  // autotuner refines them per geometry
+  t.reg_depth = 0;         // every depth < 10 in the lane's shared-memory rows (fewest instructions)
   return t;
 }
 

@@ -32,7 +32,8 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
 constexpr int kScanTile = kScanThreads * kScanPer;
 constexpr int kSlabDepth = 10;     // depths [R, 10) in a lane-private shared-memory row
-constexpr int kSlabPitch = 33;     // 32 lanes + 1 pad: rows land on distinct bank groups
+constexpr int kSlabPitch = 32;     // lane L's rows stay in bank group L % 8: a quarter-warp's row
+                                   // accesses never conflict, whatever depths its lanes hit
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
@@ -562,7 +563,7 @@ __device__ __forceinline__ void xor_bucket_global(GsBucket* p, uint64_t a, uint6
 // XOR one record {mix(k'), checksum} = q into bucket depth d of column c: registers for d < R, the
 // lane's shared-memory row for d < kSlabDepth, HBM beyond; d == bkt (or c >= C) touches nothing.
 template <int R, bool SMALL>
-__device__ __forceinline__ void apply_update(uint4 (&acc)[R], uint4* slab_g, GsBucket* skv, uint32_t c, uint32_t C,
+__device__ __forceinline__ void apply_update(uint4* acc, uint4* slab_g, GsBucket* skv, uint32_t c, uint32_t C,
                                              uint32_t bkt, uint32_t d, const uint4& q) {
   constexpr int kRows = kSlabDepth - R;
   const bool live = c < C;
@@ -665,7 +666,7 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
     }
 
     for (int i = lane; i < kSlabWords; i += 32) slab[i] = make_uint4(0, 0, 0, 0);
-    uint4 acc[CG][kRegDepth];
+    uint4 acc[CG][kRegDepth > 0 ? kRegDepth : 1];
 #pragma unroll
     for (int g = 0; g < CG; g++)
 #pragma unroll
@@ -790,6 +791,7 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
 template <int CG, bool SMALL, bool TEN>
 gs_status launch_ingest_r(gs_graph* g, uint32_t nv, cudaStream_t s) {
   switch (g->tune.reg_depth) {
+    case 0: return launch_ingest<CG, 0, SMALL, TEN>(g, nv, s);
     case 1: return launch_ingest<CG, 1, SMALL, TEN>(g, nv, s);
     case 3: return launch_ingest<CG, 3, SMALL, TEN>(g, nv, s);
     default: return launch_ingest<CG, 2, SMALL, TEN>(g, nv, s);

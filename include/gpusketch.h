@@ -190,7 +190,7 @@ gs_status gs_read_binary(const char* path, int32_t device, gs_graph** out);
 typedef struct gs_tuning {
   uint32_t chunk;            /* records per sketch-update work item (>= 32) */
   uint32_t warps_per_block;  /* warps per sketch-update block (1..16) */
-  uint32_t reg_depth;        /* bucket depths each lane keeps in registers (1..3) */
+  uint32_t reg_depth;        /* bucket depths each lane keeps in registers (0..3) */
   uint32_t reserved;
 } gs_tuning;
 /* Reads / replaces the launch parameters of the sketch-update kernel.  Results never depend on them.

@@ -305,7 +305,8 @@ def test_results_independent_of_tuning(restatement):
     star = np.stack([np.zeros(3000, np.uint32), np.arange(1, 3001, dtype=np.uint32)], 1)
     pairs = np.concatenate([rng.integers(0, V, size=(60000, 2), dtype=np.uint32), star])
     want = oracle_bytes(restatement, V, seed, pairs)
-    for chunk, warps, r in [(32, 1, 1), (1024, 4, 2), (4096, 8, 3), (100000, 16, 1), (777, 3, 2)]:
+    for chunk, warps, r in [(32, 1, 1), (1024, 4, 2), (4096, 8, 3), (100000, 16, 1), (777, 3, 2), (64, 2, 0),
+                            (5000, 16, 0)]:
         with gs.GraphSketch(V, seed) as g:
             set_tuning(g, chunk, warps, r)
             assert get_tuning(g) == {"chunk": chunk, "warps_per_block": warps, "reg_depth": r}
