@@ -3,22 +3,21 @@
 // Replaces the reference's host gutters + CudaStream double buffering + sketchUpdate kernel
 // (include/cuda_stream.h:146-276, src/cuda_kernel.cu:197-257).  One ingest pass over n records:
 //
-//   1. k_count_*    histogram of records per virtual vertex (level*V + v), warp-aggregated
-//                   with __match_any_sync so R-MAT hubs do not serialise on one counter.
-//   2. k_scan_*     exclusive scans of the record counts and of the per-vertex work-chunk
-//                   counts (ceil(count / chunk)).
-//   3. k_scatter_*  each record writes its neighbour id into its vertex's slice of d_nbr.
-//   4. k_ingest     one warp per work chunk of one vertex.  Lane c owns sketch column c: for
-//                   every record it hashes the edge for its column (XXH3 with the per-column
-//                   constant folded, gs_common.cuh) and XORs {edge, checksum} into a
-//                   warp-private shared-memory slab holding depths [0, D) of its column.
-//                   Only lane c ever touches column c, so the slab needs no atomics and the
-//                   padded [depth][33] layout keeps the 16-byte accesses bank-conflict free.
-//                   Depths >= D (probability 2^-D per record and column) XOR straight into the
-//                   HBM sketch with red.global.xor.  At the end of the chunk the non-zero slab
-//                   buckets and the deterministic bucket are merged into the vertex sketch with
-//                   coalesced 16-byte read-modify-writes (plain when the vertex is one chunk,
-//                   atomic XOR when several warps share it).
+//   1. k_part_count / k_part_scan    per block, a shared-memory histogram of the records' keys
+//                                    (level*V + v) >> lb; one global atomic per non-empty bucket
+//   2. k_part_scatter(_staged)       records placed by bucket: sorted per block in shared memory,
+//                                    then written as coalesced runs
+//   3. k_vert_count, k_scan_*        per-vertex record counts and work chunks ceil(count / chunk)
+//   4. k_vert_scatter                neighbours placed by vertex inside each chunk of a bucket
+//   5. k_ingest                      one warp per work chunk of one vertex.  Lane c owns sketch
+//                                    column c: per record it hashes the edge for its column (XXH3
+//                                    with the column constant folded, gs_common.cuh) and XORs
+//                                    {mix(edge), checksum} into its own shared-memory row for that
+//                                    depth (depths < 10); deeper buckets (probability 2^-10) go
+//                                    straight to HBM with red.global.xor.  At the end of the chunk
+//                                    the non-zero rows and the deterministic bucket are merged into
+//                                    the vertex sketch (plain read-modify-write when the vertex is
+//                                    one chunk, atomic XOR when several warps share it).
 //
 // XOR is commutative and associative, so the result is bit-identical to the reference's
 // sequential Sketch::update over the same records (src/sketch.cpp:85-99), whatever the order.
@@ -36,6 +35,12 @@ constexpr int kSlabPitch = 32;     // lane L's rows stay in bank group L % 8: a 
                                    // accesses never conflict, whatever depths its lanes hit
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Shared-memory slot counter: the old value of hist[key] (the record's place among its key's
+// records), nothing for invalid lanes.
+__device__ __forceinline__ uint32_t slot_inc(uint32_t* hist, uint32_t key, bool valid) {
+  return valid ? atomicAdd(&hist[key], 1u) : 0u;
+}
 
 struct PairTag {
   uint32_t V, num_levels, L;
@@ -212,14 +217,14 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter(const uint2* __re
   }
 }
 
-// Pass 1 placement when every edge makes exactly two records (one level): each thread keeps its
-// edges' bucket ranks in registers, the block's records are sorted by bucket in shared memory, and
-// each bucket's run is written out with consecutive threads on consecutive addresses.  The edges
-// are read once (the generic kernel above reads them twice and scatters 8-byte writes).
-constexpr int kStageEdgesPerThread = kPartEdges / kPartThreads;
-
+// Pass 1 placement when every edge makes exactly two records (one level).  Pass A counts the block's
+// records per bucket in shared memory; after the block scan and the global range
+// reservation, pass B reads the edges again (from L2: the block read them a moment ago) and takes each
+// record's place in the block's bucket-sorted shared stage from a cursor; the stage is then written
+// out with consecutive threads on consecutive addresses of each bucket's run.  Nothing is held in
+// registers across the scan.
 size_t part_scatter_staged_smem(uint32_t H) {
-  return (size_t)((3 * H + 1 + 1) & ~1u) * sizeof(uint32_t) + (size_t)2 * kPartEdges * sizeof(uint2);
+  return (size_t)((4 * H + 1 + 1) & ~1u) * sizeof(uint32_t) + (size_t)2 * kPartEdges * sizeof(uint2);
 }
 
 __global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint2* __restrict__ pairs, uint64_t n,
@@ -228,30 +233,26 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint
                                                                       uint2* __restrict__ part, uint64_t cap,
                                                                       uint32_t* __restrict__ status) {
   extern __shared__ uint32_t sh[];
-  uint32_t* hist = sh;            // [H] records per bucket, then ranks
+  uint32_t* hist = sh;            // [H] records per bucket
   uint32_t* loff = sh + H;        // [H] exclusive offsets in the block's sorted order
   uint32_t* gbase = sh + 2 * H;   // [H] first global position of the block's run of each bucket
-  uint32_t* s_total = sh + 3 * H;
-  uint2* stage = reinterpret_cast<uint2*>(sh + ((3 * H + 1 + 1) & ~1u));  // [2 * kPartEdges]
-  uint32_t* cur = bkt + 2 * H + 1;
+  uint32_t* cur = sh + 3 * H;     // [H] placement cursors
+  uint32_t* s_total = sh + 4 * H;
+  uint2* stage = reinterpret_cast<uint2*>(sh + ((4 * H + 1 + 1) & ~1u));  // [2 * kPartEdges]
+  uint32_t* gcur = bkt + 2 * H + 1;
   const uint32_t lvl = t.fixed_level >= 0 ? (uint32_t)t.fixed_level : 0u;
   for (uint32_t i = threadIdx.x; i < H; i += blockDim.x) hist[i] = 0;
   __syncthreads();
   const uint64_t e0 = (uint64_t)blockIdx.x * kPartEdges;
-  uint32_t ku[kStageEdgesPerThread], kv[kStageEdgesPerThread], ru[kStageEdgesPerThread], rv[kStageEdgesPerThread];
-#pragma unroll
-  for (int k = 0; k < kStageEdgesPerThread; k++) {
-    const uint64_t e = e0 + threadIdx.x + (uint64_t)k * kPartThreads;
-    ku[k] = 0xffffffffu;
-    if (e < n) {
-      const uint2 p = pairs[e];
-      if (p.x < t.V && p.y < t.V && p.x != p.y) {  // out-of-range records were reported by k_part_count
-        ku[k] = lvl * t.V + p.x;
-        kv[k] = lvl * t.V + p.y;
-        ru[k] = atomicAdd(&hist[ku[k] >> lb], 1u);
-        rv[k] = atomicAdd(&hist[kv[k] >> lb], 1u);
-      }
-    }
+  const uint64_t e1 = min(n, e0 + kPartEdges);
+  // out-of-range records were reported by k_part_count; self-loops cancel
+  for (uint64_t b = e0; b < e1; b += blockDim.x) {
+    const uint64_t e = b + threadIdx.x;
+    uint2 p = make_uint2(0, 0);
+    if (e < e1) p = pairs[e];
+    const bool ok = e < e1 && p.x < t.V && p.y < t.V && p.x != p.y;
+    slot_inc(hist, (lvl * t.V + p.x) >> lb, ok);
+    slot_inc(hist, (lvl * t.V + p.y) >> lb, ok);
   }
   __syncthreads();
   // exclusive scan of the block histogram: thread i owns buckets [i*per, (i+1)*per)
@@ -266,18 +267,25 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint
     for (uint32_t b = b0; b < b1; b++) {
       const uint32_t c = hist[b];
       loff[b] = run;
-      gbase[b] = c ? atomicAdd(&cur[b], c) : 0u;
+      cur[b] = run;
+      gbase[b] = c ? atomicAdd(&gcur[b], c) : 0u;
       run += c;
     }
     if (threadIdx.x == 0) *s_total = tot.x;
   }
   __syncthreads();
-#pragma unroll
-  for (int k = 0; k < kStageEdgesPerThread; k++) {
-    if (ku[k] == 0xffffffffu) continue;
-    const uint32_t nu = kv[k] - lvl * t.V, nv = ku[k] - lvl * t.V;
-    stage[loff[ku[k] >> lb] + ru[k]] = make_uint2(ku[k], nu);
-    stage[loff[kv[k] >> lb] + rv[k]] = make_uint2(kv[k], nv);
+  for (uint64_t b = e0; b < e1; b += blockDim.x) {
+    const uint64_t e = b + threadIdx.x;
+    uint2 p = make_uint2(0, 0);
+    if (e < e1) p = pairs[e];
+    const bool ok = e < e1 && p.x < t.V && p.y < t.V && p.x != p.y;
+    const uint32_t ku = lvl * t.V + p.x, kv = lvl * t.V + p.y;
+    const uint32_t pu = slot_inc(cur, ku >> lb, ok);
+    const uint32_t pv = slot_inc(cur, kv >> lb, ok);
+    if (ok) {
+      stage[pu] = make_uint2(ku, p.y);
+      stage[pv] = make_uint2(kv, p.x);
+    }
   }
   __syncthreads();
   const uint32_t total = *s_total;
@@ -357,83 +365,6 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __re
       const uint2 r = part[i];
       const uint32_t k = r.x & mask;
       const uint32_t pos = base[k] + atomicAdd(&hist[k], 1u);
-      if (pos < cap) nbr[pos] = r.y;
-      else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
-    }
-    __syncthreads();
-  }
-}
-
-// Pass 2 placement with the chunk's records sorted by vertex in shared memory first, so that every
-// vertex's run of neighbours is written by consecutive threads to consecutive addresses.
-constexpr int kVertPerThread = kVertChunk / kPartThreads;
-constexpr size_t kStagedSmemLimit = 200 * 1024;
-
-size_t vert_scatter_staged_smem(uint32_t lb) {
-  const uint32_t nk = 1u << lb;
-  return (size_t)((3 * nk + 2 + 1) & ~1u) * sizeof(uint32_t) + (size_t)kVertChunk * sizeof(uint2);
-}
-
-__global__ void __launch_bounds__(kPartThreads, 2) k_vert_scatter_staged(const uint2* __restrict__ part,
-                                                                      const uint32_t* __restrict__ bkt, uint32_t H,
-                                                                      uint32_t lb, uint32_t* __restrict__ cursor,
-                                                                      uint32_t* __restrict__ nbr, uint64_t cap,
-                                                                      uint32_t* __restrict__ status) {
-  extern __shared__ uint32_t sh[];
-  const uint32_t nk = 1u << lb, mask = nk - 1;
-  uint32_t* hist = sh;          // [nk]
-  uint32_t* loff = sh + nk;     // [nk]
-  uint32_t* gbase = sh + 2 * nk;
-  uint32_t* s_d = sh + 3 * nk;  // [2]: bucket of the chunk, records in it
-  uint2* stage = reinterpret_cast<uint2*>(sh + ((3 * nk + 2 + 1) & ~1u));
-  const uint32_t* off = bkt + H;
-  const uint32_t* choff = bkt + 3 * H + 1;
-  const uint32_t total = status[5];
-  for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
-    if (threadIdx.x == 0) s_d[0] = chunk_bucket(choff, H, c);
-    for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x) hist[i] = 0;
-    __syncthreads();
-    const uint32_t d = s_d[0];
-    const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
-    const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
-    uint32_t key[kVertPerThread], nb[kVertPerThread], rk[kVertPerThread];
-#pragma unroll
-    for (int k = 0; k < kVertPerThread; k++) {
-      const uint32_t i = r0 + threadIdx.x + (uint32_t)k * kPartThreads;
-      key[k] = 0xffffffffu;
-      if (i < r1) {
-        const uint2 r = part[i];
-        key[k] = r.x & mask;
-        nb[k] = r.y;
-        rk[k] = atomicAdd(&hist[key[k]], 1u);
-      }
-    }
-    __syncthreads();
-    {
-      const uint32_t per = (nk + blockDim.x - 1) / blockDim.x;
-      const uint32_t b0 = min(nk, threadIdx.x * per), b1 = min(nk, b0 + per);
-      uint32_t sum = 0;
-      for (uint32_t b = b0; b < b1; b++) sum += hist[b];
-      uint2 tot;
-      const uint2 ex = block_exclusive_scan(make_uint2(sum, 0u), &tot);
-      uint32_t run = ex.x;
-      for (uint32_t b = b0; b < b1; b++) {
-        const uint32_t h = hist[b];
-        loff[b] = run;
-        gbase[b] = h ? atomicAdd(&cursor[(d << lb) + b], h) : 0u;
-        run += h;
-      }
-      if (threadIdx.x == 0) s_d[1] = tot.x;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < kVertPerThread; k++)
-      if (key[k] != 0xffffffffu) stage[loff[key[k]] + rk[k]] = make_uint2(key[k], nb[k]);
-    __syncthreads();
-    const uint32_t n = s_d[1];
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint2 r = stage[i];
-      const uint64_t pos = (uint64_t)gbase[r.x] + (i - loff[r.x]);
       if (pos < cap) nbr[pos] = r.y;
       else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
     }
@@ -819,21 +750,6 @@ gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& 
   return GS_OK;
 }
 
-gs_status launch_vert_scatter_staged(const uint2* part, const uint32_t* bkt, uint32_t H, uint32_t lb, uint32_t* cursor,
-                                     uint32_t* nbr, uint64_t cap, uint32_t* status, int grid, cudaStream_t s) {
-  const size_t smem = vert_scatter_staged_smem(lb);
-  static size_t smem_set[64] = {};
-  int dev = 0;
-  GS_CUDA_TRY(cudaGetDevice(&dev));
-  if (smem_set[dev & 63] < smem) {
-    GS_CUDA_TRY(cudaFuncSetAttribute(k_vert_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    smem_set[dev & 63] = smem;
-  }
-  k_vert_scatter_staged<<<grid, kPartThreads, smem, s>>>(part, bkt, H, lb, cursor, nbr, cap, status);
-  GS_CUDA_TRY(cudaGetLastError());
-  return GS_OK;
-}
-
 }  // namespace
 
 gs_status gs_ensure_ingest_scratch(gs_graph* g, uint64_t records) {
@@ -954,13 +870,8 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
       k_vert_count<<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt,
                                                                              g->d_status);
       GS_TRY(scan_counts(g, nv, s));
-      if (vert_scatter_staged_smem(lb) <= kStagedSmemLimit) {
-        GS_TRY(launch_vert_scatter_staged(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status,
-                                          grid2, s));
-      } else {  // very large vertex spaces: the per-vertex tables of a bucket no longer fit beside the stage
-        k_vert_scatter<<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(
-            g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status);
-      }
+      k_vert_scatter<<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(
+          g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status);
       GS_CUDA_TRY(cudaGetLastError());
     }
     {
