@@ -82,6 +82,8 @@ SIGNATURES = {
     "gs_upload_sketches": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P]),
     "gs_write_binary": (C.c_int, [_P, C.c_char_p]),
     "gs_read_binary": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(_P)]),
+    "gs_set_eager_dsu": (C.c_int, [_P, C.c_int]),
+    "gs_has_cached_query": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "gs_get_tuning": (C.c_int, [_P, _P]),
     "gs_set_tuning": (C.c_int, [_P, _P]),
     "gs_profile_enable": (C.c_int, [_P, C.c_int]),

@@ -183,10 +183,18 @@ class CCGPUSketchAlg:
         return self._g.geometry.num_samples
 
     def pre_insert(self, upd: GraphUpdate, thr_id: int = 0) -> None:
-        """No eager DSU: every query runs Boruvka on the sketches (the NO_EAGER_DSU build)."""
+        """Nothing to do here: with set_eager_dsu(True) the library keeps its DSU current on every
+        ingested edge record (CCSketchAlg::pre_insert, src/cc_sketch_alg.cpp:106-131)."""
+
+    def set_eager_dsu(self, on: bool = True) -> None:
+        """Library extension: the eager DSU answers connected_components() without Boruvka while
+        no ingested record may have deleted a forest edge (off by default, like NO_EAGER_DSU)."""
+        self._g.set_eager_dsu(on)
 
     def has_cached_query(self, query_code: int) -> bool:
-        return False
+        if query_code != QueryCode.CONNECTIVITY:
+            return False
+        return self._g.has_cached_query()
 
     def print_configuration(self) -> None:
         print(self.config)

@@ -48,8 +48,17 @@ class CCGPUSketchAlg {
   void allocate_worker_memory(size_t num_workers) { (void)num_workers; }
   size_t get_desired_updates_per_batch() { return gs_desired_updates_per_batch(g); }
   node_id_t get_num_vertices() { return num_vertices; }
-  void pre_insert(GraphUpdate, int = 0) {}           // no eager DSU: queries always run Boruvka
-  bool has_cached_query(int) { return false; }
+  // With set_eager_dsu(true) the library keeps the DSU current on every ingested edge record, so
+  // pre_insert has nothing left to do; has_cached_query reports whether connected_components() will
+  // be answered without Boruvka (include/cc_sketch_alg.h:185-191).
+  void pre_insert(GraphUpdate, int = 0) {}
+  bool has_cached_query(int query_code) {
+    if (query_code != CONNECTIVITY) return false;
+    int cached = 0;
+    gs_throw_if(gs_has_cached_query(g, &cached), "gs_has_cached_query");
+    return cached != 0;
+  }
+  void set_eager_dsu(bool on) { gs_throw_if(gs_set_eager_dsu(g, on ? 1 : 0), "gs_set_eager_dsu"); }
   void print_configuration() { std::cout << config << std::endl; }
 
   void apply_update_batch(int thr_id, node_id_t src_vertex, const std::vector<node_id_t>& dst_vertices) {

@@ -35,6 +35,7 @@
 // DSU: CAS hooking of the larger root under the smaller (include/dsu.h:155-167 unions by random
 // priority instead), so every component's root is its minimum vertex id and labels are deterministic;
 // every walk is bounded by V+64 steps and reports GS_DEV_ERR_DSU_LIMIT.
+#include "gs_dsu.cuh"
 #include "gs_internal.h"
 
 namespace {
@@ -47,9 +48,6 @@ constexpr uint64_t kBarrierWaitNs = 1000000000ull;  // a barrier wait gives up a
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
-__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
-  return *reinterpret_cast<const volatile uint32_t*>(p);
-}
 
 // loads of data written by other blocks earlier in the same launch bypass L1
 __device__ __forceinline__ GsBucket ld_bucket_cg(const GsBucket* p) {
@@ -92,48 +90,6 @@ __device__ __forceinline__ void sample_warp(const GsBucket* col, const GsBucket*
   }
   *code = kFail;
   *idx = 0;
-}
-
-// Root of x.  Path halving: every visited vertex is re-pointed at its grandparent.  Only roots are
-// ever CAS'd and a non-root stays a non-root, so these plain stores only ever move a pointer up
-// to another ancestor.
-__device__ __forceinline__ uint32_t dsu_find(uint32_t* parent, uint32_t x, uint32_t limit, uint32_t* err) {
-  volatile uint32_t* P = parent;
-  for (uint32_t it = 0; it < limit; it++) {
-    const uint32_t p = P[x];
-    if (p == x) return x;
-    const uint32_t gp = P[p];
-    if (gp != p) P[x] = gp;
-    x = gp;
-  }
-  atomicOr(err, (uint32_t)GS_DEV_ERR_DSU_LIMIT);
-  return x;
-}
-
-// Root of x without writing anything: the compress phase, where each parent[v] must have exactly
-// one writer (thread v).  A path-halving store from another thread could otherwise land after v's
-// root and leave v pointing at a non-root.
-__device__ __forceinline__ uint32_t dsu_root(const uint32_t* parent, uint32_t x, uint32_t limit, uint32_t* err) {
-  for (uint32_t it = 0; it < limit; it++) {
-    const uint32_t p = ld_volatile(parent + x);
-    if (p == x) return x;
-    x = p;
-  }
-  atomicOr(err, (uint32_t)GS_DEV_ERR_DSU_LIMIT);
-  return x;
-}
-
-// union of global vertices a, b; true when it joined two components
-__device__ __forceinline__ bool dsu_union(uint32_t* parent, uint32_t a, uint32_t b, uint32_t limit, uint32_t* err) {
-  for (uint32_t it = 0; it < limit; it++) {
-    a = dsu_find(parent, a, limit, err);
-    b = dsu_find(parent, b, limit, err);
-    if (a == b) return false;
-    if (a < b) { const uint32_t t = a; a = b; b = t; }
-    if (atomicCAS(&parent[a], a, b) == a) return true;
-  }
-  atomicOr(err, (uint32_t)GS_DEV_ERR_DSU_LIMIT);
-  return false;
 }
 
 // Grid-wide barrier of a co-resident launch.  Returns false when any block gave up waiting.  The

@@ -29,6 +29,9 @@ void gs_free_graph(gs_graph* g) {
   cudaFree(g->d_status);
   cudaFree(g->d_parent); cudaFree(g->d_size); cudaFree(g->d_res); cudaFree(g->d_samp); cudaFree(g->d_acc);
   cudaFree(g->d_forest);
+  cudaFree(g->d_eager_set);
+  cudaFree(g->d_eager_status);
+  if (g->h_eager) cudaFreeHost(g->h_eager);
   for (int i = 0; i < 2; i++) {
     if (g->ev_copy[i]) cudaEventDestroy(g->ev_copy[i]);
     if (g->ev_done[i]) cudaEventDestroy(g->ev_done[i]);
@@ -180,7 +183,7 @@ gs_status gs_clear(gs_graph* g) {
   GS_CUDA_TRY(cudaMemsetAsync(g->d_sk, 0, bytes, g->stream));
   g->labels_valid = false;
   std::fill(g->sample_cursor.begin(), g->sample_cursor.end(), 0u);
-  return GS_OK;
+  return gs_eager_reset_empty(g, g->stream);
 }
 
 gs_status gs_graph_set_stream(gs_graph* g, void* stream) {
@@ -318,7 +321,15 @@ gs_status gs_connected_components(gs_graph* g, uint32_t level, uint32_t* labels,
   GS_GUARD(g);
   cudaStream_t s = g->stream;
   GS_TRY(check_status(g, s));
-  GS_TRY(gs_boruvka(g, level, 0, s));
+  bool cached = false;
+  if (level == 0) GS_TRY(gs_eager_state(g, s, &cached));
+  if (cached) {
+    GS_TRY(gs_eager_answer(g, s));   // CCSketchAlg::connected_components with shared_dsu_valid
+  } else {
+    GS_TRY(gs_boruvka(g, level, 0, s));
+    g->last_answer_eager = false;
+    if (level == 0) GS_TRY(gs_eager_rebuild(g, s));
+  }
   if (rounds) *rounds = g->last_rounds;
   if (labels || num_cc) {
     std::vector<uint32_t> tmp;
@@ -351,6 +362,7 @@ gs_status gs_spanning_forest(gs_graph* g, uint32_t level, uint32_t* edges, uint6
   if (!g || !edges || !num_edges) { gs_set_error("gs_spanning_forest: null argument"); return GS_ERR_BAD_ARG; }
   GS_TRY(gs_connected_components(g, level, nullptr, nullptr, nullptr));
   GS_GUARD(g);
+  if (g->last_answer_eager) GS_TRY(gs_eager_forest(g, g->stream));  // the eager forest, as the reference returns
   *num_edges = g->last_forest_edges;
   GS_CUDA_TRY(cudaMemcpy(edges, g->d_forest, (size_t)2 * g->last_forest_edges * sizeof(uint32_t),
                          cudaMemcpyDeviceToHost));
@@ -392,6 +404,7 @@ gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, 
   cudaFree(d_all);
   for (uint32_t j = done; j < k; j++) sizes[j] = 0;
   g->labels_valid = false;
+  gs_eager_invalidate(g, s);  // the parent array now holds the last forest's partition
   if (st != GS_OK) return st;
   if (st2 != GS_OK) return st2;
   GS_CUDA_TRY(cudaGetLastError());
@@ -445,7 +458,7 @@ gs_status gs_upload_sketches(gs_graph* g, uint32_t level, uint32_t first, uint32
   GS_CUDA_TRY(cudaMemcpy(g->d_sk + ((size_t)level * g->V + first) * nb, host_in, (size_t)count * nb * sizeof(GsBucket),
                          cudaMemcpyHostToDevice));
   g->labels_valid = false;
-  return GS_OK;
+  return gs_eager_invalidate(g, g->stream);
 }
 
 gs_status gs_write_binary(gs_graph* g, const char* path) {
@@ -526,6 +539,23 @@ gs_status gs_gen_rmat_stream(uint32_t log2_v, double a, double b, double c, doub
 }
 
 }  // extern "C"
+
+// ---- eager DSU ----
+
+extern "C" gs_status gs_set_eager_dsu(gs_graph* g, int enable) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  DeviceGuard guard(g->device);
+  return gs_eager_enable(g, enable != 0, g->stream);
+}
+
+extern "C" gs_status gs_has_cached_query(gs_graph* g, int* cached) {
+  if (!g || !cached) { gs_set_error("null argument"); return GS_ERR_BAD_ARG; }
+  DeviceGuard guard(g->device);
+  bool v = false;
+  GS_TRY(gs_eager_state(g, g->stream, &v));
+  *cached = v ? 1 : 0;
+  return GS_OK;
+}
 
 // ---- tuning ----
 

@@ -878,6 +878,7 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
       GsProfScope ps(g, GS_PROF_INGEST, s, 1);
       GS_TRY(ingest_chunks(g, nv, s));
     }
+    if (fixed_level < 0) GS_TRY(gs_eager_ingest(g, reinterpret_cast<const uint32_t*>(p), m, s));
     g->records_total += m;
     done += m;
   }
@@ -888,6 +889,8 @@ gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* 
                                    const uint64_t* d_starts, const uint64_t* d_sizes, uint32_t nbat,
                                    const uint32_t* d_dsts, cudaStream_t s) {
   if (nbat == 0) return GS_OK;
+  // directed one-sided updates: the eager DSU cannot follow them
+  GS_TRY(gs_eager_invalidate(g, s));
   const uint32_t nv = g->num_levels * g->V;
   GS_TRY(gs_ensure_ingest_scratch(g, 1));
   GS_CUDA_TRY(cudaMemsetAsync(g->d_cnt, 0, (size_t)(nv + 1) * sizeof(uint32_t), s));

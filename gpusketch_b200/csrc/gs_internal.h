@@ -16,6 +16,14 @@ struct GsIngTenant {
   uint32_t V, C, bkt, nb, pad;
 };
 
+// One entry of the eager DSU's forest set: an edge id (0 = empty), the ingest batch that added it,
+// and how often that batch toggled it.
+struct GsEagerSlot {
+  uint64_t key;
+  uint32_t epoch;
+  uint32_t count;
+};
+
 // Ingest tuning knobs (picked per geometry by gs_tune_for; overridable through
 // gs_set_tuning for the autotuner).
 struct GsTuning {
@@ -87,6 +95,16 @@ struct gs_graph {
   bool labels_valid = false;     // d_parent holds the partition of the last query
   uint32_t labels_level = 0;
 
+  // ---- eager DSU (gs_eager.cu): connectivity kept current by the ingest path ----
+  bool eager_on = false;
+  bool last_answer_eager = false;     // the last CC answer came from the eager DSU, not Boruvka
+  GsEagerSlot* d_eager_set = nullptr; // forest edge set, eager_mask + 1 slots
+  uint32_t* d_eager_status = nullptr; // [0] invalid (non-zero) [1] error bits [2] scratch counter
+  uint32_t* h_eager = nullptr;        // pinned mirror of the status words
+  uint32_t eager_mask = 0;
+  uint32_t eager_epoch = 0;
+  uint64_t eager_answers = 0;
+
   // ---- profiling ----
   bool prof_on = false;
   bool capturing = false;                // launches are being recorded into a CUDA graph: no event timing
@@ -143,6 +161,16 @@ gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* 
                                    uint32_t nb, const uint32_t* d_dsts, cudaStream_t s);
 // Device Boruvka on one level; forest edges stay in g->d_forest.
 gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s);
+
+// Eager DSU (gs_eager.cu).
+gs_status gs_eager_enable(gs_graph* g, bool on, cudaStream_t s);
+gs_status gs_eager_reset_empty(gs_graph* g, cudaStream_t s);           // the empty graph: valid, no forest
+gs_status gs_eager_invalidate(gs_graph* g, cudaStream_t s);            // the next query runs Boruvka
+gs_status gs_eager_ingest(gs_graph* g, const uint32_t* d_pairs, uint64_t n, cudaStream_t s);
+gs_status gs_eager_state(gs_graph* g, cudaStream_t s, bool* valid);    // synchronizes
+gs_status gs_eager_answer(gs_graph* g, cudaStream_t s);                // labels from the DSU
+gs_status gs_eager_rebuild(gs_graph* g, cudaStream_t s);               // after a Boruvka query
+gs_status gs_eager_forest(gs_graph* g, cudaStream_t s);                // the eager forest into d_forest
 
 // One independent graph of a Boruvka launch (gs_boruvka.cu).
 struct GsBorTenant {

@@ -166,6 +166,16 @@ class GraphSketch:
               "gs_min_cut")
         return value.value, lvl.value, cut.value, side
 
+    # ---- eager DSU ----
+    def set_eager_dsu(self, on: bool = True) -> None:
+        """Keep a device DSU current during ingest so that queries skip Boruvka while it is valid."""
+        check(self._lib.gs_set_eager_dsu(self._h, int(on)), "gs_set_eager_dsu")
+
+    def has_cached_query(self) -> bool:
+        out = C.c_int()
+        check(self._lib.gs_has_cached_query(self._h, C.byref(out)), "gs_has_cached_query")
+        return bool(out.value)
+
     # ---- profiling ----
     def profile_enable(self, on: bool = True) -> None:
         check(self._lib.gs_profile_enable(self._h, int(on)), "gs_profile_enable")

@@ -186,6 +186,20 @@ gs_status gs_upload_sketches(gs_graph* g, uint32_t level, uint32_t first_vertex,
 gs_status gs_write_binary(gs_graph* g, const char* path);
 gs_status gs_read_binary(const char* path, int32_t device, gs_graph** out);
 
+/* ---- eager DSU / cached connectivity ----
+ * With the eager DSU on, every ingest keeps a device DSU and spanning forest of the stream next to
+ * the sketches, and gs_connected_components answers from them - without Boruvka - until a record may
+ * have deleted a forest edge; the next query then runs Boruvka and rebuilds them from its forest
+ * (CCSketchAlg::pre_insert, src/cc_sketch_alg.cpp:106-131; connected_components :542-549).  Records
+ * of a batch are applied concurrently, so a batch that toggles an edge it has just made a forest
+ * edge also invalidates.  Connected-components graphs only; off by default (the reference's
+ * NO_EAGER_DSU build), because streams with frequent deletions pay the passes and rarely profit.
+ * gs_ingest_vertex_batches and gs_upload_sketches invalidate; gs_clear resets to the empty graph. */
+gs_status gs_set_eager_dsu(gs_graph* g, int enable);
+/* has_cached_query(CONNECTIVITY) (include/cc_sketch_alg.h:185-191): 1 when the next
+ * gs_connected_components will be answered from the eager DSU.  Synchronizes the handle. */
+gs_status gs_has_cached_query(gs_graph* g, int* cached);
+
 /* ---- tuning (set by the autotuner, gpusketch_b200/autotune.py) ---- */
 typedef struct gs_tuning {
   uint32_t chunk;            /* records per sketch-update work item (>= 32) */
