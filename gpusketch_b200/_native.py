@@ -78,6 +78,7 @@ SIGNATURES = {
     "gs_disjoint_spanning_forests": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P]),
     "gs_min_cut": (C.c_int, [_P, C.c_uint32, _U64P, _U32P, _U64P, _P]),
     "gs_exact_min_cut": (C.c_int, [C.c_uint32, _P, C.c_uint64, _U64P, _P]),
+    "gs_edge_store_edges": (C.c_int, [_P, C.c_uint32, _P, C.c_uint64, _U64P]),
     "gs_download_sketches": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P]),
     "gs_upload_sketches": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P]),
     "gs_write_binary": (C.c_int, [_P, C.c_char_p]),

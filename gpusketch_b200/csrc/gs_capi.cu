@@ -29,6 +29,9 @@ void gs_free_graph(gs_graph* g) {
   cudaFree(g->d_status);
   cudaFree(g->d_parent); cudaFree(g->d_size); cudaFree(g->d_res); cudaFree(g->d_samp); cudaFree(g->d_acc);
   cudaFree(g->d_forest);
+  cudaFree(g->d_store);
+  cudaFree(g->d_store_status);
+  if (g->h_store) cudaFreeHost(g->h_store);
   cudaFree(g->d_eager_set);
   cudaFree(g->d_eager_status);
   if (g->h_eager) cudaFreeHost(g->h_eager);
@@ -183,6 +186,7 @@ gs_status gs_clear(gs_graph* g) {
   GS_CUDA_TRY(cudaMemsetAsync(g->d_sk, 0, bytes, g->stream));
   g->labels_valid = false;
   std::fill(g->sample_cursor.begin(), g->sample_cursor.end(), 0u);
+  GS_TRY(gs_store_clear(g, g->stream));
   return gs_eager_reset_empty(g, g->stream);
 }
 
@@ -424,14 +428,45 @@ gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_f
       cert.insert(cert.end(), edges.begin() + (size_t)f * 2 * (V - 1),
                   edges.begin() + (size_t)f * 2 * (V - 1) + 2 * sizes[f]);
     const uint64_t cut = gs_exact_min_cut_host(V, cert.data(), cert.size() / 2, side);
-    if (cut < k || lvl + 1 == g->num_levels) {
+    if (cut < k || (lvl + 1 == g->num_levels && !gs_store_active(g))) {
       *value = cut << lvl;
       if (level_found) *level_found = lvl;
       if (cut_at_level) *cut_at_level = cut;
       return GS_OK;
     }
   }
-  return GS_ERR_INTERNAL;
+  // no sketched level certified a cut below k: the first unsketched level, from the exact tier,
+  // answers whatever its value (tools/min_cut.cu:221-247)
+  const uint32_t lvl = g->num_levels;
+  {
+    GS_GUARD(g);
+    GS_TRY(check_status(g, g->stream));
+    std::vector<uint32_t> exact;
+    GS_TRY(gs_store_edges(g, lvl, &exact, g->stream));
+    const std::vector<uint32_t> cert = gs_k_forest_certificate(V, exact, k);
+    const uint64_t cut = gs_exact_min_cut_host(V, cert.data(), cert.size() / 2, side);
+    *value = cut << lvl;
+    if (level_found) *level_found = lvl;
+    if (cut_at_level) *cut_at_level = cut;
+  }
+  return GS_OK;
+}
+
+gs_status gs_edge_store_edges(gs_graph* g, uint32_t min_tag, uint32_t* edges, uint64_t capacity, uint64_t* num_edges) {
+  if (!g || !num_edges || (capacity && !edges)) { gs_set_error("gs_edge_store_edges: bad arguments"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  GS_TRY(check_status(g, g->stream));
+  std::vector<uint32_t> exact;
+  GS_TRY(gs_store_edges(g, min_tag, &exact, g->stream));
+  std::vector<uint64_t> ids(exact.size() / 2);
+  for (size_t i = 0; i < ids.size(); i++) ids[i] = ((uint64_t)exact[2 * i] << 32) | exact[2 * i + 1];
+  std::sort(ids.begin(), ids.end());
+  *num_edges = ids.size();
+  for (size_t i = 0; i < ids.size() && i < capacity; i++) {
+    edges[2 * i] = (uint32_t)(ids[i] >> 32);
+    edges[2 * i + 1] = (uint32_t)ids[i];
+  }
+  return GS_OK;
 }
 
 gs_status gs_download_sketches(gs_graph* g, uint32_t level, uint32_t first, uint32_t count, void* host_out) {

@@ -878,7 +878,10 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
       GsProfScope ps(g, GS_PROF_INGEST, s, 1);
       GS_TRY(ingest_chunks(g, nv, s));
     }
-    if (fixed_level < 0) GS_TRY(gs_eager_ingest(g, reinterpret_cast<const uint32_t*>(p), m, s));
+    if (fixed_level < 0) {
+      GS_TRY(gs_eager_ingest(g, reinterpret_cast<const uint32_t*>(p), m, s));
+      GS_TRY(gs_store_ingest(g, reinterpret_cast<const uint32_t*>(p), m, s));
+    }
     g->records_total += m;
     done += m;
   }

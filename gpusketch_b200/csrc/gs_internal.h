@@ -24,6 +24,14 @@ struct GsEagerSlot {
   uint32_t count;
 };
 
+// One entry of the exact tier of deep min-cut levels (gs_store.cu): an edge id (0 = empty), its
+// subgraph tag and the parity of its toggles (odd = present).
+struct GsStoreSlot {
+  uint64_t key;
+  uint32_t tag;
+  uint32_t parity;
+};
+
 // Ingest tuning knobs (picked per geometry by gs_tune_for; overridable through
 // gs_set_tuning for the autotuner).
 struct GsTuning {
@@ -105,6 +113,12 @@ struct gs_graph {
   uint32_t eager_epoch = 0;
   uint64_t eager_answers = 0;
 
+  // ---- exact tier of the deep min-cut levels (gs_store.cu) ----
+  GsStoreSlot* d_store = nullptr;     // allocated at the first tagged ingest that needs it
+  uint32_t* d_store_status = nullptr; // [1] error bits [2] slots used [3] scratch counter
+  uint32_t* h_store = nullptr;        // pinned mirror
+  uint32_t store_mask = 0;
+
   // ---- profiling ----
   bool prof_on = false;
   bool capturing = false;                // launches are being recorded into a CUDA graph: no event timing
@@ -172,6 +186,12 @@ gs_status gs_eager_answer(gs_graph* g, cudaStream_t s);                // labels
 gs_status gs_eager_rebuild(gs_graph* g, cudaStream_t s);               // after a Boruvka query
 gs_status gs_eager_forest(gs_graph* g, cudaStream_t s);                // the eager forest into d_forest
 
+// Exact tier of the deep min-cut levels (gs_store.cu).
+bool gs_store_active(const gs_graph* g);                               // tags can reach past the sketches
+gs_status gs_store_ingest(gs_graph* g, const uint32_t* d_pairs, uint64_t n, cudaStream_t s);
+gs_status gs_store_clear(gs_graph* g, cudaStream_t s);
+gs_status gs_store_edges(gs_graph* g, uint32_t min_tag, std::vector<uint32_t>* out, cudaStream_t s);
+
 // One independent graph of a Boruvka launch (gs_boruvka.cu).
 struct GsBorTenant {
   uint64_t sk_off;      // bucket offset of the tenant's vertex-0 sketch from the launch's sketch base
@@ -204,6 +224,8 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s);
 
 // Exact global min cut (host), gs_mincut.cpp.
 uint64_t gs_exact_min_cut_host(uint32_t V, const uint32_t* pairs, uint64_t m, uint8_t* side);
+// k maximal edge-disjoint spanning forests of an edge list (gs_mincut.cpp), as interleaved pairs.
+std::vector<uint32_t> gs_k_forest_certificate(uint32_t V, const std::vector<uint32_t>& edges, uint32_t k);
 
 // R-MAT record generator shared by host and device (gs_gen.cu).
 gs_status gs_gen_rmat_device(uint32_t log2_v, double a, double b, double c, double delete_frac,

@@ -166,6 +166,15 @@ class GraphSketch:
               "gs_min_cut")
         return value.value, lvl.value, cut.value, side
 
+    def edge_store_edges(self, min_tag: int | None = None) -> np.ndarray:
+        """Present edges of the exact tier with subgraph tag >= min_tag (default: num_levels)."""
+        t = self.num_levels if min_tag is None else min_tag
+        n = C.c_uint64()
+        check(self._lib.gs_edge_store_edges(self._h, t, None, 0, C.byref(n)), "gs_edge_store_edges")
+        out = np.empty((max(n.value, 1), 2), np.uint32)
+        check(self._lib.gs_edge_store_edges(self._h, t, out.ctypes.data, n.value, C.byref(n)), "gs_edge_store_edges")
+        return out[: n.value].copy()
+
     # ---- eager DSU ----
     def set_eager_dsu(self, on: bool = True) -> None:
         """Keep a device DSU current during ingest so that queries skip Boruvka while it is valid."""

@@ -162,8 +162,10 @@ gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, 
 
 /* Min-cut driver of the reference's tools/min_cut.cu:208-252: for level g = 0,1,... take k
  * disjoint spanning forests, compute the exact minimum cut of their union, and stop at the
- * first level whose cut is < k (or at the last level).  value = cut * 2^g.  side (host,
- * length V, may be NULL) receives 1 for vertices on one side of the cut. */
+ * first level whose cut is < k.  When no sketched level does and tags can pass the sketches
+ * (num_subgraphs > num_levels), level g = num_levels answers from the exact tier (see
+ * gs_edge_store_edges) whatever its value; otherwise the last sketched level answers.
+ * value = cut * 2^g.  side (host, length V, may be NULL) receives 1 for vertices on one side. */
 gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_found,
                      uint64_t* cut_at_level, uint8_t* side);
 
@@ -171,6 +173,14 @@ gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_f
  * Replaces the VieCut call of MCSketchAlg::calc_minimum_cut (src/mc_sketch_alg.cpp:966-1002). */
 gs_status gs_exact_min_cut(uint32_t num_vertices, const uint32_t* pairs, uint64_t num_edges,
                            uint64_t* value, uint8_t* side);
+
+/* The exact tier of a min-cut graph (EdgeStore, src/edge_store.cpp:60-300; get_edges): edges whose
+ * subgraph tag reaches num_levels are also kept exactly on the device, with each toggle flipping
+ * their presence; gs_min_cut answers from them when no sketched level certifies a cut below k.
+ * Writes the present edges with tag >= min_tag (sorted by edge id, at most `capacity`) and their
+ * count to *num_edges.  Empty when num_subgraphs <= num_levels (no tag passes the sketches). */
+gs_status gs_edge_store_edges(gs_graph* g, uint32_t min_tag, uint32_t* edges, uint64_t capacity,
+                              uint64_t* num_edges);
 
 /* Copy vertex sketches [first, first+count) of `level` to / from host memory in the
  * contiguous [vertex][num_buckets] Bucket layout of Sketch::serialize

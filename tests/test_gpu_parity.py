@@ -341,3 +341,47 @@ def test_min_cut_full_config():
     assert (value, level, cut_at) == (3, 0, 3)
     s = side.astype(bool)
     assert s[:n].all() != s[n:].all() and (s[:n].all() or not s[:n].any()) and (s[n:].all() or not s[n:].any())
+
+
+def test_edge_store_tier_holds_the_deep_levels(restatement):
+    """Edges whose subgraph tag passes the sketched levels are kept exactly (toggles flip them)."""
+    V, seed, levels, L = 700, 23, 2, 19
+    rng = np.random.default_rng(41)
+    pairs = rng.integers(0, V, size=(40000, 2), dtype=np.uint32)
+    pairs = np.concatenate([pairs, pairs[:5000]])            # some edges toggled back out
+    with gs.GraphSketch(V, seed, num_levels=levels, num_subgraphs=L) as g:
+        g.ingest_pairs(pairs[:20000])
+        g.ingest_pairs(pairs[20000:])
+        for t in (levels, levels + 2):
+            got = g.edge_store_edges(t)
+            final = restatement.final_edges(V, pairs)
+            tags = np.array([(gs.hash64((int(a) << 32) | int(b), seed) | (1 << (L - 1))) for a, b in final.tolist()],
+                            dtype=np.uint64)
+            depth = np.array([(int(x) & -int(x)).bit_length() - 1 for x in tags])
+            want = final[depth >= t]
+            want = want[np.lexsort((want[:, 1], want[:, 0]))]
+            assert np.array_equal(got, want), t
+        g.clear()
+        assert len(g.edge_store_edges()) == 0
+
+
+def test_min_cut_falls_back_to_the_exact_tier():
+    """One sketched level and a cut of 6 > k=4: level 0 certifies no cut below k, so the first
+    unsketched level answers from the exact tier: its certificate cut times 2."""
+    n, seed = 120, 0x5EED0004
+    rng = np.random.default_rng(14)
+    blocks = []
+    for off in (0, n):
+        a, b = np.triu_indices(n, 1)
+        keep = rng.random(a.size) < 0.5
+        blocks.append(np.stack([a[keep] + off, b[keep] + off], 1))
+    cross = np.stack([rng.integers(0, n, 6), rng.integers(n, 2 * n, 6)], 1)
+    pairs = np.concatenate(blocks + [cross]).astype(np.uint32)
+    V, L = 2 * n, 15
+    with gs.GraphSketch(V, seed, num_levels=1, num_subgraphs=L) as g:
+        g.ingest_pairs(pairs)
+        value, level, cut_at, side = g.min_cut(4)
+        assert level == 1 and value == cut_at * 2
+        exact = g.edge_store_edges(1)
+        lam, _ = gs.exact_min_cut(V, exact)
+        assert min(lam, 4) <= cut_at <= lam                  # the k-forest certificate of level 1
