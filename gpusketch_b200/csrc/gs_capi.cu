@@ -435,16 +435,16 @@ gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_f
       return GS_OK;
     }
   }
-  // no sketched level certified a cut below k: the first unsketched level, from the exact tier,
-  // answers whatever its value (tools/min_cut.cu:221-247)
+  // no sketched level certified a cut below k: the first unsketched level answers whatever its
+  // value, with the exact minimum cut of all its edges from the exact tier (tools/min_cut.cu:221-247;
+  // get_adjlist_spanning_forests returns the store's whole edge list, src/mc_gpu_sketch_alg.cpp:207-209)
   const uint32_t lvl = g->num_levels;
   {
     GS_GUARD(g);
     GS_TRY(check_status(g, g->stream));
     std::vector<uint32_t> exact;
     GS_TRY(gs_store_edges(g, lvl, &exact, g->stream));
-    const std::vector<uint32_t> cert = gs_k_forest_certificate(V, exact, k);
-    const uint64_t cut = gs_exact_min_cut_host(V, cert.data(), cert.size() / 2, side);
+    const uint64_t cut = gs_exact_min_cut_host(V, exact.data(), exact.size() / 2, side);
     *value = cut << lvl;
     if (level_found) *level_found = lvl;
     if (cut_at_level) *cut_at_level = cut;

@@ -224,8 +224,6 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s);
 
 // Exact global min cut (host), gs_mincut.cpp.
 uint64_t gs_exact_min_cut_host(uint32_t V, const uint32_t* pairs, uint64_t m, uint8_t* side);
-// k maximal edge-disjoint spanning forests of an edge list (gs_mincut.cpp), as interleaved pairs.
-std::vector<uint32_t> gs_k_forest_certificate(uint32_t V, const std::vector<uint32_t>& edges, uint32_t k);
 
 // R-MAT record generator shared by host and device (gs_gen.cu).
 gs_status gs_gen_rmat_device(uint32_t log2_v, double a, double b, double c, double delete_frac,

@@ -189,41 +189,3 @@ extern "C" gs_status gs_exact_min_cut(uint32_t num_vertices, const uint32_t* pai
   *value = gs_exact_min_cut_host(num_vertices, pairs, num_edges, side);
   return GS_OK;
 }
-
-// k edge-disjoint maximal spanning forests of a multigraph, chosen in edge-id order: forest f takes
-// every remaining edge that joins two of its components.  Their union keeps every cut of fewer than
-// k edges exactly, and every larger cut at k edges or more (Nagamochi-Ibaraki), which is the
-// certificate the min-cut driver reads (tools/min_cut.cu:221-247; get_adjlist_spanning_forests).
-std::vector<uint32_t> gs_k_forest_certificate(uint32_t V, const std::vector<uint32_t>& edges, uint32_t k) {
-  std::vector<uint64_t> rest(edges.size() / 2);
-  for (size_t i = 0; i < rest.size(); i++) {
-    const uint32_t a = std::min(edges[2 * i], edges[2 * i + 1]), b = std::max(edges[2 * i], edges[2 * i + 1]);
-    rest[i] = ((uint64_t)a << 32) | b;
-  }
-  std::sort(rest.begin(), rest.end());
-  std::vector<uint32_t> cert;
-  std::vector<uint32_t> parent(V);
-  auto find = [&](uint32_t x) {
-    while (parent[x] != x) {
-      parent[x] = parent[parent[x]];
-      x = parent[x];
-    }
-    return x;
-  };
-  for (uint32_t f = 0; f < k && !rest.empty(); f++) {
-    for (uint32_t v = 0; v < V; v++) parent[v] = v;
-    std::vector<uint64_t> left;
-    for (const uint64_t e : rest) {
-      const uint32_t a = find((uint32_t)(e >> 32)), b = find((uint32_t)e);
-      if (a == b) {
-        left.push_back(e);
-      } else {
-        parent[std::max(a, b)] = std::min(a, b);
-        cert.push_back((uint32_t)(e >> 32));
-        cert.push_back((uint32_t)e);
-      }
-    }
-    rest.swap(left);
-  }
-  return cert;
-}

@@ -164,7 +164,8 @@ gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, 
  * disjoint spanning forests, compute the exact minimum cut of their union, and stop at the
  * first level whose cut is < k.  When no sketched level does and tags can pass the sketches
  * (num_subgraphs > num_levels), level g = num_levels answers from the exact tier (see
- * gs_edge_store_edges) whatever its value; otherwise the last sketched level answers.
+ * gs_edge_store_edges) with the exact min cut of all its edges, whatever its value; otherwise
+ * the last sketched level answers.
  * value = cut * 2^g.  side (host, length V, may be NULL) receives 1 for vertices on one side. */
 gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_found,
                      uint64_t* cut_at_level, uint8_t* side);
