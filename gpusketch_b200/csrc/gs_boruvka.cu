@@ -22,14 +22,15 @@
 // Per round (five grid barriers):
 //   sizes       component sizes from the compressed parent array (warp-aggregated atomics); the
 //               size array also freezes the round's root set for sampling and unions
-//   accumulate  warps walk runs of consecutive vertices and XOR column r + the deterministic bucket
-//               into a register accumulator per component, flushed with red.global.xor when the
-//               component changes (one flush per run once a giant component forms)
-//   sample      a warp finds 32 roots at a time with one ballot, then samples each: lane j checks
-//               bucket j (and j+32) with one XXH3 each (Bucket_Boruvka::is_good, include/bucket.h:
-//               65-67); the deterministic bucket is zero / good first, else the first good bucket by
-//               depth (Sketch::sample, src/sketch.cpp:110-132); the component's accumulator row is
-//               zeroed once read, so rows are all zero between rounds and between launches
+//   accumulate  warps take runs of vertices from a shared counter, stage the members' column r and
+//               deterministic bucket in shared memory with cp.async, and XOR them into a register
+//               accumulator per component, flushed with red.global.xor when the component changes
+//   sample      round 0: every vertex samples its own sketch (an octet of lanes per vertex for one
+//               graph, a thread per vertex for many); later rounds: one warp per listed root, lane j
+//               checking bucket j (and j+32) with one XXH3 each (Bucket_Boruvka::is_good,
+//               include/bucket.h:65-67).  The deterministic bucket is zero / good first, else the first
+//               good bucket by depth (Sketch::sample, src/sketch.cpp:110-132); the component's
+//               accumulator row is zeroed once read, so rows are all zero between rounds and launches
 //   union       one thread per root unions its sampled edge, so thousands of DSU walks overlap
 //   compress    full path compression, sizes cleared, per-tenant stop / out-of-samples decisions
 // DSU: CAS hooking of the larger root under the smaller (include/dsu.h:155-167 unions by random
@@ -42,6 +43,7 @@ namespace {
 
 constexpr uint32_t kGood = 0, kZero = 1, kFail = 2;
 constexpr uint32_t kAccRun = 16;                 // vertices a warp stages in shared memory at once
+constexpr uint32_t kAccGrab = 64;                // vertices a warp takes from the shared work counter
 constexpr uint32_t kThreads = 256;
 constexpr uint32_t kWarps = kThreads / 32;
 constexpr uint64_t kBarrierWaitNs = 1000000000ull;  // a barrier wait gives up after about a second
@@ -90,6 +92,64 @@ __device__ __forceinline__ void sample_warp(const GsBucket* col, const GsBucket*
   }
   *code = kFail;
   *idx = 0;
+}
+
+// Sketch::sample by one thread (round 0 of multi-graph launches, whose vertices are mostly sparse
+// and decide at the deterministic bucket): the column by depth, four buckets per batch of loads.
+__device__ __forceinline__ void sample_thread(const GsBucket* col, const GsBucket* det, uint32_t bkt, uint64_t csmix,
+                                              uint32_t* code, uint64_t* idx) {
+  const GsBucket d = ld_bucket_cg(det);
+  if (d.alpha == 0 && d.gamma == 0) { *code = kZero; *idx = 0; return; }
+  if (is_good(d, csmix)) { *code = kGood; *idx = d.alpha; return; }
+  for (uint32_t j0 = 0; j0 < bkt; j0 += 4) {
+    GsBucket b[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) b[k] = j0 + k < bkt ? ld_bucket_cg(col + j0 + k) : GsBucket{0, 0};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if (j0 + k < bkt && is_good(b[k], csmix)) {
+        *code = kGood;
+        *idx = b[k].alpha;
+        return;
+      }
+    }
+  }
+  *code = kFail;
+  *idx = 0;
+}
+
+// Sketch::sample by an octet of lanes (round 0, where every vertex samples its own sketch: four
+// vertices per warp).  Lane k of the octet checks depths k, k+8, ...; an octet's answer is the lowest
+// good depth among its lanes.  The octets of a warp may belong to graphs with different bkt, so the
+// pass count is the warp's largest bkt: every lane runs the same passes and reaches every
+// full-warp collective.
+__device__ __forceinline__ void sample_octet(const GsBucket* col, const GsBucket* det, uint32_t bkt, uint64_t csmix,
+                                             bool active, uint32_t* code, uint64_t* idx) {
+  const uint32_t lane = lane_id(), sub = lane & 7u, oct = lane >> 3;
+  bool decided = !active;
+  *code = kFail;
+  *idx = 0;
+  if (active) {
+    const GsBucket d = ld_bucket_cg(det);
+    if (d.alpha == 0 && d.gamma == 0) { *code = kZero; decided = true; }
+    else if (is_good(d, csmix)) { *code = kGood; *idx = d.alpha; decided = true; }
+  }
+  const uint32_t bmax = __reduce_max_sync(0xffffffffu, bkt);
+  for (uint32_t j0 = 0; j0 < bmax; j0 += 8) {
+    if (__all_sync(0xffffffffu, decided)) break;
+    const uint32_t j = j0 + sub;
+    GsBucket b = GsBucket{0, 0};
+    const bool look = !decided && j < bkt;
+    if (look) b = ld_bucket_cg(col + j);
+    const uint32_t m = __ballot_sync(0xffffffffu, look && is_good(b, csmix));
+    const uint32_t mine = (m >> (8u * oct)) & 0xffu;
+    const uint64_t a = __shfl_sync(0xffffffffu, b.alpha, mine ? 8u * oct + (uint32_t)(__ffs(mine) - 1) : lane);
+    if (!decided && mine) {
+      *code = kGood;
+      *idx = a;
+      decided = true;
+    }
+  }
 }
 
 // Grid-wide barrier of a co-resident launch.  Returns false when any block gave up waiting.  The
@@ -144,6 +204,7 @@ struct BorArgs {
   uint32_t* forest;            // [2 * forest_cap]
   uint32_t forest_cap;
   uint32_t* status;            // [0] error bits [3] roots [4] forest edges [5] active tenants [6,7] barrier
+                               // [12] accumulate work counter
   uint32_t* tstate;            // [T][4]: done, modified this round, rounds, out of samples
 };
 
@@ -177,6 +238,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
   GsBucket* stage = reinterpret_cast<GsBucket*>(smem + ((A.T + 3u) & ~3u)) + (threadIdx.x >> 5) * kAccRun * A.W;
   uint32_t* err = A.status;
   uint32_t* nroots_p = A.status + 3;
+  uint32_t* acc_next = A.status + 12;  // accumulate work counter, zero at launch and after every round
   uint32_t* bcount = A.status + 6;
   uint32_t* bgen = A.status + 7;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
@@ -215,17 +277,23 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
       if (!grid_sync(bcount, bgen, err)) return;
 
       // ---- accumulate column r + the deterministic bucket per component ----
-      // Each warp owns a contiguous slice of vertices and walks it kAccRun at a time: the columns of
-      // the run's members are copied into shared memory with cp.async (all in flight together), then
-      // folded in vertex order into a register accumulator that is flushed with red.global.xor when
-      // the component changes.  A vertex whose root is another vertex is in a component of two or
-      // more, so only roots read their own size: no load hammers a giant component's root.
+      // Warps take runs of kAccGrab vertices from a shared counter (finished tenants' vertices cost
+      // almost nothing, so fixed slices would leave most warps idle at the barrier) and walk each
+      // run kAccRun at a time: the columns of the members are copied into shared memory with
+      // cp.async (all in flight together), then folded in vertex order into a register accumulator
+      // that is flushed with red.global.xor when the component changes.  A vertex whose root is
+      // another vertex is in a component of two or more, so only roots read their own size: no load
+      // hammers a giant component's root.
       {
-        const uint32_t per = ((span + gwarps - 1) / gwarps + kAccRun - 1) / kAccRun * kAccRun;
-        const uint32_t w0 = A.vlo + min(span, gwarp * per), w1 = A.vlo + min(span, gwarp * per + per);
         uint32_t cur = 0xffffffffu, w = 0;
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
-        for (uint32_t start = w0; start < w1; start += kAccRun) {
+        for (;;) {
+          uint32_t g0 = 0;
+          if (lane == 0) g0 = atomicAdd(acc_next, kAccGrab);
+          g0 = __shfl_sync(0xffffffffu, g0, 0);
+          if (g0 >= span) break;
+          const uint32_t w1 = A.vlo + min(span, g0 + kAccGrab);
+        for (uint32_t start = A.vlo + g0; start < w1; start += kAccRun) {
           const uint32_t n = min(kAccRun, w1 - start);
           uint32_t rt = 0xffffffffu, tt = 0;
           if (lane < n) {
@@ -270,6 +338,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
           }
           __syncwarp();
         }
+        }
         if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
       }
       if (!grid_sync(bcount, bgen, err)) return;
@@ -279,7 +348,63 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
     // The accumulator row of a sampled component is zeroed after reading, so every row is zero
     // again when the round ends (and at the start of the next launch).
     const uint32_t nroots = round == 0 ? span : ld_volatile(nroots_p);
-    for (uint32_t k = gwarp; k < nroots; k += gwarps) {
+    if (round == 0 && A.T > 1) {
+      // every vertex samples its own sketch: one thread each (many sparse graphs)
+      for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) {
+        const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
+        if (s_done[t]) continue;
+        const GsBorTenant& T = tenant_of(A, t);
+        const uint32_t col = T.round0_col;
+        if (col >= T.ns) {  // OutOfSamplesException
+          A.tstate[4 * t + 3] = 1u;
+          continue;
+        }
+        const GsBucket* own = A.sk + T.sk_off + (size_t)(v - T.vbase) * T.nb;
+        uint32_t code;
+        uint64_t idx;
+        sample_thread(own + (size_t)col * T.bkt, own + (T.nb - 1), T.bkt, T.csmix, &code, &idx);
+        uint64_t e = ~0ull;
+        if (code == kFail) {
+          A.tstate[4 * t + 1] = 1u;
+        } else if (code == kGood) {
+          const uint32_t s = (uint32_t)(idx >> 32), d = (uint32_t)idx;
+          if (s < T.V && d < T.V && s != d) e = ((uint64_t)(T.vbase + s) << 32) | (T.vbase + d);
+        }
+        A.samp[v] = e;
+      }
+    } else if (round == 0) {
+      // every vertex samples its own sketch: an octet of lanes each, four vertices per warp (one
+      // graph, whose high-degree vertices find their first good bucket deep in the column)
+      for (uint32_t base = A.vlo + gwarp * 4u; base < A.V; base += gwarps * 4u) {
+        const uint32_t v = base + (lane >> 3);
+        bool active = v < A.V;
+        uint32_t t = 0;
+        if (active) {
+          t = A.vtenant ? A.vtenant[v] : 0u;
+          active = !s_done[t];
+        }
+        const GsBorTenant& T = tenant_of(A, active ? t : 0u);
+        const uint32_t col = T.round0_col;
+        const bool oos = active && col >= T.ns;  // OutOfSamplesException
+        if (oos && (lane & 7u) == 0) A.tstate[4 * t + 3] = 1u;
+        const GsBucket* own = A.sk + T.sk_off + (size_t)((active ? v : T.vbase) - T.vbase) * T.nb;
+        uint32_t code;
+        uint64_t idx;
+        sample_octet(own + (size_t)(oos ? 0u : col) * T.bkt, own + (T.nb - 1), T.bkt, T.csmix, active && !oos, &code,
+                     &idx);
+        if (active && !oos && (lane & 7u) == 0) {
+          uint64_t e = ~0ull;
+          if (code == kFail) {
+            A.tstate[4 * t + 1] = 1u;
+          } else if (code == kGood) {
+            const uint32_t s = (uint32_t)(idx >> 32), d = (uint32_t)idx;
+            if (s < T.V && d < T.V && s != d) e = ((uint64_t)(T.vbase + s) << 32) | (T.vbase + d);
+          }
+          A.samp[v] = e;
+        }
+      }
+    }
+    for (uint32_t k = gwarp; round > 0 && k < nroots; k += gwarps) {
       const uint32_t v = round == 0 ? A.vlo + k : __ldcg(&A.roots[k]);
       const uint32_t t = A.vtenant ? A.vtenant[v] : 0u;
       if (s_done[t]) continue;
@@ -341,7 +466,10 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
       A.parent[v] = dsu_root(A.parent, v, limit, err);
       A.size[v] = 0;
     }
-    if (gtid == 0) *nroots_p = 0;
+    if (gtid == 0) {
+      *nroots_p = 0;
+      *acc_next = 0;
+    }
     for (uint32_t t = gtid; t < A.T; t += gthreads) {
       volatile uint32_t* ts = A.tstate + 4 * t;
       if (ts[0]) continue;
