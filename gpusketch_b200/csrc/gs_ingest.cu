@@ -615,8 +615,25 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
       rec[lane] = make_uint4((uint32_t)E, (uint32_t)(E >> 32), (uint32_t)cs, (uint32_t)(cs >> 32));
       __syncwarp();
       const uint32_t cnt = min(32u, re - b);
-      // two records per iteration: their hash chains are independent and overlap in the pipeline
+      // four (then two, then one) records per iteration: their hash chains are independent and
+      // overlap in the pipeline
       uint32_t j = 0;
+      for (; j + 3 < cnt; j += 4) {
+        const uint4 q0 = rec[j], q1 = rec[j + 1], q2 = rec[j + 2], q3 = rec[j + 3];
+        const uint64_t E0 = ((uint64_t)q0.y << 32) | q0.x, E1 = ((uint64_t)q1.y << 32) | q1.x;
+        const uint64_t E2 = ((uint64_t)q2.y << 32) | q2.x, E3 = ((uint64_t)q3.y << 32) | q3.x;
+#pragma unroll
+        for (int g = 0; g < CG; g++) {
+          const uint32_t d0 = gs_depth_from_mixed(E0 ^ cmix[g], bkt);
+          const uint32_t d1 = gs_depth_from_mixed(E1 ^ cmix[g], bkt);
+          const uint32_t d2 = gs_depth_from_mixed(E2 ^ cmix[g], bkt);
+          const uint32_t d3 = gs_depth_from_mixed(E3 ^ cmix[g], bkt);
+          apply_update<R, SMALL>(acc[g], slab + g * kRows * kSlabPitch, skv, lane + 32u * g, C, bkt, d0, q0);
+          apply_update<R, SMALL>(acc[g], slab + g * kRows * kSlabPitch, skv, lane + 32u * g, C, bkt, d1, q1);
+          apply_update<R, SMALL>(acc[g], slab + g * kRows * kSlabPitch, skv, lane + 32u * g, C, bkt, d2, q2);
+          apply_update<R, SMALL>(acc[g], slab + g * kRows * kSlabPitch, skv, lane + 32u * g, C, bkt, d3, q3);
+        }
+      }
       for (; j + 1 < cnt; j += 2) {
         const uint4 q0 = rec[j], q1 = rec[j + 1];
         const uint64_t E0 = ((uint64_t)q0.y << 32) | q0.x, E1 = ((uint64_t)q1.y << 32) | q1.x;
