@@ -521,7 +521,7 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
   const size_t smem = (size_t)((L.T + 3u) & ~3u) * sizeof(uint32_t) + (size_t)kWarps * kAccRun * L.W * sizeof(GsBucket);
   // occupancy depends on the shared-memory size: cache it per (device, size)
   struct Occ { size_t smem = 0; int blocks = 0; };
-  static Occ occ[64];
+  static thread_local Occ occ[64];  // per host thread: handles may be used from several threads at once
   Occ& o = occ[dev < 64 ? dev : 63];
   if (o.smem != smem) {
     GS_CUDA_TRY(cudaFuncSetAttribute(k_boruvka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

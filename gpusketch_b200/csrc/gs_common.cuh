@@ -127,12 +127,20 @@ GsGeom gs_make_geom(uint32_t V, double sketches_factor);
 // Thread-local error message behind gs_last_error().
 void gs_set_error(const std::string& msg);
 
+// the file name of a source path, for error messages
+inline const char* gs_source_name(const char* path) {
+  const char* base = path;
+  for (const char* p = path; *p; ++p)
+    if (*p == '/') base = p + 1;
+  return base;
+}
+
 #define GS_CUDA_TRY(expr)                                                                    \
   do {                                                                                       \
     cudaError_t _e = (expr);                                                                 \
     if (_e != cudaSuccess) {                                                                 \
-      gs_set_error(std::string(#expr) + ": " + cudaGetErrorString(_e) + " @" + __FILE__ +     \
-                   ":" + std::to_string(__LINE__));                                          \
+      gs_set_error(std::string(#expr) + ": " + cudaGetErrorString(_e) + " @" +                \
+                   gs_source_name(__FILE__) + ":" + std::to_string(__LINE__));               \
       return _e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA;                     \
     }                                                                                        \
   } while (0)

@@ -719,7 +719,7 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   // the opt-in shared-memory limit is a per-device function attribute; the persistent grid fills
   // every SM with as many blocks as registers and shared memory allow
   struct Cache { size_t smem = 0; int warps = 0; int blocks = 0; };
-  static Cache cache[64];  // per device, per kernel instantiation
+  static thread_local Cache cache[64];  // per host thread, device and kernel instantiation
   Cache& cc = cache[g->device < 64 ? g->device : 63];
   if (cc.smem != smem || cc.warps != warps) {
     GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest<CG, R, SMALL, TEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -754,7 +754,7 @@ gs_status launch_ingest_s(gs_graph* g, uint32_t nv, bool small, cudaStream_t s) 
 gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& t, uint32_t lb, uint32_t H,
                                      uint32_t* bkt, uint2* part, uint64_t cap, uint32_t* status, cudaStream_t s) {
   const size_t smem = part_scatter_staged_smem(H);
-  static size_t smem_set[64] = {};
+  static thread_local size_t smem_set[64] = {};
   int dev = 0;
   GS_CUDA_TRY(cudaGetDevice(&dev));
   if (smem_set[dev & 63] < smem) {
