@@ -43,7 +43,7 @@ def set_tuning(g, chunk: int, warps_per_block: int, reg_depth: int) -> None:
     check(_fns(g)[1](g._h, C.byref(t)), "set_tuning")
 
 
-def autotune(g, sample_pairs, chunks=(256, 512, 1024, 2048), warps=(8, 16), reg_depths=(0, 1),
+def autotune(g, sample_pairs, chunks=(256, 512, 1024, 2048), warps=(8, 12, 16), reg_depths=(0, 1),
              repeats: int = 2, table: list | None = None) -> dict:
     """Times every candidate on `sample_pairs` (a CUDA tensor of records) and applies the fastest.
     The sketches are restored afterwards: each candidate ingests the sample twice (XOR cancels)."""
@@ -69,7 +69,7 @@ def autotune(g, sample_pairs, chunks=(256, 512, 1024, 2048), warps=(8, 16), reg_
     return {"chunk": best[0], "warps_per_block": best[1], "reg_depth": best[2], "ingest_ms": best_ms / (2 * repeats)}
 
 
-def autotune_engine(e, slice_tenants, slice_offsets, pairs, chunks=(128, 256, 512, 1024), warps=(4, 8, 16),
+def autotune_engine(e, slice_tenants, slice_offsets, pairs, chunks=(128, 256, 512, 1024), warps=(4, 8, 12, 16),
                     reg_depths=(0, 1), repeats: int = 1, table: list | None = None) -> dict:
     """Engine variant: times the multi-tenant sketch update on one batch of device-resident slices
     (ingested twice per candidate, so the tenants' sketches are unchanged) and applies the fastest.

@@ -109,6 +109,26 @@ __device__ __forceinline__ uint32_t gs_depth_from_mixed(uint64_t x, uint32_t max
   if (__builtin_expect(flo == 0u, 0)) d = 32u + __clz(__brev(h2 ^ (h2 >> 28)));
   return d < max_depth ? d : max_depth;
 }
+
+// The same depth in two steps, for loops that branch on the depth anyway.  gs_depth_low returns the
+// ctz of the final hash's low word (32 when that word is zero, probability 2^-32), exact whenever it
+// is below 32, and the high product word in *h2; gs_depth_finish completes a low-word depth of 32
+// from the high word and caps it at max_depth.
+__device__ __forceinline__ uint32_t gs_depth_low(uint64_t x, uint32_t* h2_out) {
+  uint64_t h = x * kGsMx2;
+  uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
+  lo ^= __umulhi(hi, 1u << 29) + 8u;
+  h = ((uint64_t)hi << 32) | lo;
+  h *= kGsMx2;
+  const uint32_t l2 = (uint32_t)h, h2 = (uint32_t)(h >> 32);
+  *h2_out = h2;
+  return __clz(__brev(l2 ^ (h2 * 16u) ^ __umulhi(l2, 16u)));
+}
+
+__device__ __forceinline__ uint32_t gs_depth_finish(uint32_t d_low, uint32_t h2, uint32_t max_depth) {
+  const uint32_t d = d_low < 32u ? d_low : 32u + __clz(__brev(h2 ^ (h2 >> 28)));
+  return d < max_depth ? d : max_depth;
+}
 #endif
 
 // ----------------------------------------------------------------------------------------

@@ -484,7 +484,53 @@ struct IngestArgs {
   uint32_t nv, V, C, bkt, nb, chunk;
   const uint32_t* vtenant;       // tenant of every vertex (tenant variant only)
   const GsIngTenant* tenants;    // geometry and arena offset of every tenant (tenant variant only)
+  uint32_t warp_words;           // shared memory per warp in uint4 (packed variant only)
 };
+
+// ---- packed lane layout (sketches of at most 24 columns) ----
+//
+// With one column per lane, a sketch of C < 32 columns leaves 32 - C lanes idle on every record
+// (8 of 32 at V = 2^17).  The packed layout gives those spare lanes the fourth record of every group
+// of four: a group takes kPackRounds = 3 rounds, in which
+//   * main lane c < C takes column c of records 0, 1, 2 of the group;
+//   * spare lane C + i (i < se = ceil(C / 3) <= 32 - C) takes column i + j se of record 3 in round j
+//     (nothing when that column is >= C).
+// A full batch of 32 staged records takes 24 rounds instead of 32 at C = 24.  Record offset, column
+// constant and row block of every (lane, round) are fixed per geometry and held in registers, so a
+// round costs one hash and one row update like the one-record-per-round loop.  Every lane XORs only
+// into rows of its own, so rounds need no synchronisation: main lane c keeps rows [depth][c] (pitch
+// p1 = C rounded up to 8), spare lane C + i keeps rows [j][depth][lane % 8] (pitch 8; se <= 8, so the
+// spare lanes' residues are distinct).  A lane's entry sits at lane % 8 of its row, so a
+// quarter-warp's accesses stay in distinct bank groups whatever depths its lanes hit.  At the end of
+// a chunk column c gathers its main row and spare slot c / se of lane C + c % se.  Records left over
+// after the groups of four (and every record of a wider sketch) take one round each on the main lanes.
+constexpr uint32_t kPackRounds = 3;
+constexpr uint32_t kPackMaxCols = 24;  // ceil(C / 3) <= 32 - C
+constexpr uint32_t kRecWords = 32;
+// at most 12 warps per block, two blocks per SM: with 8 KB of rows per warp shared memory holds 24
+// warps per SM, and the register cap that two 384-thread blocks leave (85) avoids spills
+constexpr int kPackMaxThreads = 384;
+
+GS_HD uint32_t pack_spare_lanes(uint32_t C) { return C <= kPackMaxCols ? (C + kPackRounds - 1) / kPackRounds : 0u; }
+GS_HD uint32_t pack_p1(uint32_t C) { return (C + 7u) & ~7u; }
+
+// uint4 words per warp: rows of the main lanes and of the spare slots, then the staged records
+GS_HD uint32_t pack_warp_words(uint32_t C) {
+  return (uint32_t)kSlabDepth * (pack_p1(C) + (pack_spare_lanes(C) ? kPackRounds * 8u : 0u)) + kRecWords;
+}
+
+__device__ __forceinline__ uint32_t chunk_owner(const IngestArgs& A, uint32_t ch, uint32_t lane) {
+  uint32_t lo = 0, hi = A.nv;
+  while (hi - lo > 1) {
+    const uint32_t step = (hi - lo + 31) / 32;
+    const uint32_t probe = lo + (lane + 1) * step;
+    const bool le = probe < hi && A.choff[probe] <= ch;
+    const uint32_t k = __popc(__ballot_sync(0xffffffffu, le));
+    lo = lo + k * step;
+    hi = min(hi, lo + step);
+  }
+  return lo;
+}
 
 __device__ __forceinline__ void xor_bucket_global(GsBucket* p, uint64_t a, uint64_t g) {
   atomicXor(reinterpret_cast<unsigned long long*>(&p->alpha), (unsigned long long)a);
@@ -555,17 +601,7 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
 
   for (uint32_t ch = gw; ch < total; ch += nw) {
-    // owner vertex: the largest vv with choff[vv] <= ch (32-way search across the warp)
-    uint32_t lo = 0, hi = A.nv;
-    while (hi - lo > 1) {
-      const uint32_t step = (hi - lo + 31) / 32;
-      const uint32_t probe = lo + (lane + 1) * step;
-      const bool le = probe < hi && A.choff[probe] <= ch;
-      const uint32_t k = __popc(__ballot_sync(0xffffffffu, le));
-      lo = lo + k * step;
-      hi = min(hi, lo + step);
-    }
-    const uint32_t vv = lo;
+    const uint32_t vv = chunk_owner(A, ch, lane);
     const uint32_t c0 = A.choff[vv];
     const bool exclusive = (A.choff[vv + 1] - c0) == 1;
     const uint32_t rb = A.off[vv] + (ch - c0) * A.chunk;
@@ -704,6 +740,183 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
   }
 }
 
+// Sketch update with the packed lane layout (reg_depth 0, at most 32 columns); chunk lookup, record
+// staging, deep-bucket path and merge as in k_ingest.
+template <bool SMALL, bool TEN>
+__global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const IngestArgs A) {
+  extern __shared__ uint4 smem[];
+  constexpr uint32_t kRows = kSlabDepth;
+  constexpr uint32_t J = kPackRounds;
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+  uint4* const wbase = smem + (size_t)wib * A.warp_words;
+  uint4* const rec = wbase + A.warp_words - kRecWords;
+
+  uint32_t C = 0, bkt = A.bkt, nb = A.nb, se = 0, p1 = 8;
+  const uint32_t V = A.V;
+  uint64_t csmix = 0, cmix = 0;
+  // per lane and round of a group: record offset, column constant, row block, column (or >= C: none)
+  uint32_t ro[J], sb[J], col[J], pitch = 0;
+  uint64_t cm[J];
+  auto set_geometry = [&](uint32_t c_new, const uint64_t* cmt) {
+    C = c_new;
+    se = pack_spare_lanes(C);
+    p1 = pack_p1(C);
+    csmix = cmt[C];
+    cmix = lane < C ? cmt[lane] : 0ull;
+    const bool main = lane < C, spare = !main && lane < C + se;
+    pitch = main ? p1 : 8u;
+#pragma unroll
+    for (uint32_t j = 0; j < J; j++) {
+      ro[j] = main ? j : J;
+      col[j] = main ? lane : (spare ? lane - C + j * se : 0xffffffffu);
+      col[j] = col[j] < C ? col[j] : 0xffffffffu;
+      cm[j] = col[j] < C ? cmt[col[j]] : 0ull;
+      sb[j] = main ? lane : kRows * p1 + (j * kRows) * 8u + (lane & 7u);
+    }
+  };
+  uint32_t cur_t = 0xffffffffu;
+  if (!TEN) set_geometry(A.C, A.colmix);
+
+  const uint32_t total = A.status[2];
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+
+  for (uint32_t ch = gw; ch < total; ch += nw) {
+    const uint32_t vv = chunk_owner(A, ch, lane);
+    const uint32_t c0ff = A.choff[vv];
+    const bool exclusive = (A.choff[vv + 1] - c0ff) == 1;
+    const uint32_t rb = A.off[vv] + (ch - c0ff) * A.chunk;
+    const uint32_t re = min(A.off[vv + 1], rb + A.chunk);
+    uint32_t v, vb = 0;
+    GsBucket* skv;
+    if (TEN) {
+      const uint32_t t = A.vtenant[vv];
+      const GsIngTenant T = A.tenants[t];
+      if (t != cur_t) {
+        cur_t = t;
+        bkt = T.bkt;
+        nb = T.nb;
+        set_geometry(T.C, A.colmix + (size_t)t * kColStride);
+      }
+      vb = T.vbase;
+      v = vv - vb;
+      skv = A.sk + T.sk_off + (size_t)v * nb;
+    } else {
+      v = vv % V;
+      skv = A.sk + (size_t)vv * nb;
+    }
+
+    const uint32_t zw = kRows * (p1 + (se ? J * 8u : 0u));
+    for (uint32_t i = lane; i < zw; i += 32) wbase[i] = make_uint4(0, 0, 0, 0);
+    uint64_t det_m = 0, det_g = 0;
+    __syncwarp();
+
+    // 32-bit shared-window addresses: row block bb of this warp at ws + 16 bb, record k at rs + 16 k
+    const uint32_t ws = (uint32_t)__cvta_generic_to_shared(wbase);
+    const uint32_t rs = (uint32_t)__cvta_generic_to_shared(rec);
+    const uint32_t pitch16 = pitch * 16u;
+    // XOR record q into the lane's column cc at the depth whose low-word part is dl (high product
+    // word h2), rows at row block bb.  Depths below kRows (and below bkt_per_col, which only a SMALL
+    // geometry has under kRows) go to the lane's rows; the rest is the rare HBM path, which also
+    // completes a depth whose low word was zero.
+    auto update = [&](bool live, uint32_t bb, uint32_t cc, uint32_t dl, uint32_t h2, const uint4& q) {
+      const uint32_t d = SMALL ? min(dl, bkt) : dl;
+      if (live && d < (SMALL ? bkt : kRows)) {
+        const uint32_t a = ws + bb * 16u + d * pitch16;
+        uint4 t;
+        asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(t.x), "=r"(t.y), "=r"(t.z), "=r"(t.w) : "r"(a));
+        t.x ^= q.x; t.y ^= q.y; t.z ^= q.z; t.w ^= q.w;
+        asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" :: "r"(a), "r"(t.x), "r"(t.y), "r"(t.z), "r"(t.w)
+                     : "memory");
+      } else if (!SMALL && live) {
+        const uint32_t dd = gs_depth_finish(dl, h2, bkt);
+        if (dd < bkt)
+          xor_bucket_global(skv + (size_t)cc * bkt + dd, gs_key_unmix(((uint64_t)q.y << 32) | q.x),
+                            ((uint64_t)q.w << 32) | q.z);
+      }
+    };
+    auto lds = [](uint32_t a) {
+      uint4 q;
+      asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(q.x), "=r"(q.y), "=r"(q.z), "=r"(q.w) : "r"(a));
+      return q;
+    };
+    auto emix = [](const uint4& q) { return ((uint64_t)q.y << 32) | q.x; };
+
+    for (uint32_t b = rb; b < re; b += 32) {
+      const uint32_t r = b + lane;
+      const bool valid = r < re;
+      const uint32_t u = valid ? A.nbr[r] - vb : v;
+      const uint64_t E = gs_key_mix(gs_concat(v, u));
+      const uint64_t cs = gs_hash_tail(E ^ csmix);
+      if (valid) { det_m ^= E; det_g ^= cs; }
+      rec[lane] = make_uint4((uint32_t)E, (uint32_t)(E >> 32), (uint32_t)cs, (uint32_t)(cs >> 32));
+      __syncwarp();
+      const uint32_t cnt = min(32u, re - b);
+      const uint32_t ng = se ? cnt >> 2 : 0u;
+      uint32_t k = 0;
+      // groups of four records; a0..a2: this lane's record of each round
+      uint32_t a0 = rs + ro[0] * 16u, a1 = rs + ro[1] * 16u, a2 = rs + ro[2] * 16u;
+      for (uint32_t gi = 0; gi < ng; gi++, k += J + 1, a0 += 16u * (J + 1), a1 += 16u * (J + 1), a2 += 16u * (J + 1)) {
+        const uint4 q0 = lds(a0), q1 = lds(a1), q2 = lds(a2);
+        uint32_t h0, h1, h2;
+        const uint32_t d0 = gs_depth_low(emix(q0) ^ cm[0], &h0);
+        const uint32_t d1 = gs_depth_low(emix(q1) ^ cm[1], &h1);
+        const uint32_t d2 = gs_depth_low(emix(q2) ^ cm[2], &h2);
+        update(col[0] < C, sb[0], col[0], d0, h0, q0);
+        update(col[1] < C, sb[1], col[1], d1, h1, q1);
+        update(col[2] < C, sb[2], col[2], d2, h2, q2);
+      }
+      // the rest: one record per round on the main lanes
+      const bool main = lane < C;
+      for (; k + 1 < cnt; k += 2) {
+        const uint4 q0 = lds(rs + 16u * k), q1 = lds(rs + 16u * (k + 1));
+        uint32_t h0, h1;
+        const uint32_t d0 = gs_depth_low(emix(q0) ^ cmix, &h0);
+        const uint32_t d1 = gs_depth_low(emix(q1) ^ cmix, &h1);
+        update(main, lane, lane, d0, h0, q0);
+        update(main, lane, lane, d1, h1, q1);
+      }
+      if (k < cnt) {
+        const uint4 q0 = lds(rs + 16u * k);
+        uint32_t h0;
+        const uint32_t d0 = gs_depth_low(emix(q0) ^ cmix, &h0);
+        update(main, lane, lane, d0, h0, q0);
+      }
+      __syncwarp();
+    }
+
+    // merge: item i -> column i / kRows, depth i % kRows, so consecutive lanes cover contiguous
+    // buckets of one column; a column's spare slot (if any) is folded in first
+    for (uint32_t i = lane; i < C * kRows; i += 32) {
+      const uint32_t cl = i / kRows, row = i % kRows;
+      uint4 t = wbase[row * p1 + cl];
+      if (se) {
+        const uint32_t j = cl / se, sl = C + (cl - j * se);
+        const uint4 t2 = wbase[kRows * p1 + (j * kRows + row) * 8u + (sl & 7u)];
+        t.x ^= t2.x; t.y ^= t2.y; t.z ^= t2.z; t.w ^= t2.w;
+      }
+      if (row >= bkt || (t.x | t.y | t.z | t.w) == 0u) continue;
+      const uint64_t a = gs_key_unmix(((uint64_t)t.y << 32) | t.x), gm = ((uint64_t)t.w << 32) | t.z;
+      GsBucket* p = skv + (size_t)cl * bkt + row;
+      if (exclusive) { p->alpha ^= a; p->gamma ^= gm; }
+      else xor_bucket_global(p, a, gm);
+    }
+    // deterministic bucket (last bucket of the sketch)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      det_m ^= __shfl_xor_sync(0xffffffffu, det_m, o);
+      det_g ^= __shfl_xor_sync(0xffffffffu, det_g, o);
+    }
+    if (lane == 0 && (det_m | det_g) != 0ull) {
+      GsBucket* p = skv + (nb - 1);
+      const uint64_t a = gs_key_unmix(det_m);
+      if (exclusive) { p->alpha ^= a; p->gamma ^= det_g; }
+      else xor_bucket_global(p, a, det_g);
+    }
+    __syncwarp();
+  }
+}
+
 size_t ingest_smem_bytes(int cg, int r, int warps) {
   return (size_t)warps * (size_t)(cg * (kSlabDepth - r) * kSlabPitch + 32) * sizeof(uint4);
 }
@@ -714,6 +927,7 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   A.off = g->d_off; A.choff = g->d_choff; A.nbr = g->d_nbr; A.sk = g->d_sk; A.colmix = g->d_colmix;
   A.status = g->d_status; A.nv = nv; A.V = g->V; A.C = g->geom.num_columns;
   A.bkt = g->geom.bkt_per_col; A.nb = g->geom.num_buckets; A.chunk = g->tune.chunk;
+  A.warp_words = 0;
   const int warps = (int)g->tune.warps_per_block;
   const size_t smem = ingest_smem_bytes(CG, R, warps);
   // the opt-in shared-memory limit is a per-device function attribute; the persistent grid fills
@@ -736,10 +950,48 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   return GS_OK;
 }
 
+// shared memory per warp of the packed kernel: the graph's geometry, or the widest need over every
+// column count up to the engine's widest tenant
+uint32_t packed_warp_words(const gs_graph* g) {
+  if (!g->d_ten) return pack_warp_words(g->geom.num_columns);
+  uint32_t w = 0;
+  for (uint32_t c = 1; c <= g->ten_max_cols && c <= 32u; c++) w = std::max(w, pack_warp_words(c));
+  return w;
+}
+
+template <bool SMALL, bool TEN>
+gs_status launch_ingest_packed(gs_graph* g, uint32_t nv, cudaStream_t s) {
+  IngestArgs A;
+  A.off = g->d_off; A.choff = g->d_choff; A.nbr = g->d_nbr; A.sk = g->d_sk; A.colmix = g->d_colmix;
+  A.status = g->d_status; A.nv = nv; A.V = g->V; A.C = g->geom.num_columns;
+  A.bkt = g->geom.bkt_per_col; A.nb = g->geom.num_buckets; A.chunk = g->tune.chunk;
+  A.vtenant = TEN ? g->d_vtenant : nullptr;
+  A.tenants = TEN ? g->d_ten : nullptr;
+  A.warp_words = packed_warp_words(g);
+  const int warps = std::min(kPackMaxThreads / 32, (int)g->tune.warps_per_block);
+  const size_t smem = (size_t)warps * A.warp_words * sizeof(uint4);
+  struct Cache { size_t smem = 0; int warps = 0; int blocks = 0; };
+  static thread_local Cache cache[64];  // per host thread, device and kernel instantiation
+  Cache& cc = cache[g->device < 64 ? g->device : 63];
+  if (cc.smem != smem || cc.warps != warps) {
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest_packed<SMALL, TEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nb = 0;
+    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest_packed<SMALL, TEN>, warps * 32, smem));
+    cc.smem = smem;
+    cc.warps = warps;
+    cc.blocks = nb > 0 ? nb : 1;
+  }
+  k_ingest_packed<SMALL, TEN><<<g->num_sms * cc.blocks, warps * 32, smem, s>>>(A);
+  GS_CUDA_TRY(cudaGetLastError());
+  return GS_OK;
+}
+
 template <int CG, bool SMALL, bool TEN>
 gs_status launch_ingest_r(gs_graph* g, uint32_t nv, cudaStream_t s) {
   switch (g->tune.reg_depth) {
-    case 0: return launch_ingest<CG, 0, SMALL, TEN>(g, nv, s);
+    case 0:
+      if constexpr (CG == 1) return launch_ingest_packed<SMALL, TEN>(g, nv, s);
+      else return launch_ingest<CG, 0, SMALL, TEN>(g, nv, s);
     case 1: return launch_ingest<CG, 1, SMALL, TEN>(g, nv, s);
     case 3: return launch_ingest<CG, 3, SMALL, TEN>(g, nv, s);
     default: return launch_ingest<CG, 2, SMALL, TEN>(g, nv, s);
@@ -951,6 +1203,7 @@ gs_status launch_ingest_scratch(const GsScratchIngest& x, cudaStream_t s) {
   A.bkt = x.geom.bkt_per_col; A.nb = x.geom.num_buckets; A.chunk = x.chunk;
   A.vtenant = nullptr;
   A.tenants = nullptr;
+  A.warp_words = 0;
   const size_t smem = ingest_smem_bytes(CG, 1, (int)x.warps);
   int nb = 0;
   GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, 1, SMALL, false>, (int)x.warps * 32, smem));

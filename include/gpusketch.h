@@ -214,8 +214,10 @@ gs_status gs_has_cached_query(gs_graph* g, int* cached);
 /* ---- tuning (set by the autotuner, gpusketch_b200/autotune.py) ---- */
 typedef struct gs_tuning {
   uint32_t chunk;            /* records per sketch-update work item (>= 32) */
-  uint32_t warps_per_block;  /* warps per sketch-update block (1..16) */
-  uint32_t reg_depth;        /* bucket depths each lane keeps in registers (0..3) */
+  uint32_t warps_per_block;  /* warps per sketch-update block (1..16; the packed layout runs at most 12) */
+  uint32_t reg_depth;        /* bucket depths each lane keeps in registers (0..3); 0 on a sketch of at
+                                most 32 columns selects the packed layout, in which lanes left over by
+                                the columns take columns of further records */
   uint32_t reserved;
 } gs_tuning;
 /* Reads / replaces the launch parameters of the sketch-update kernel.  Results never depend on them.
