@@ -454,7 +454,7 @@ def run_gs(args):
     peak, peak_kind = measured_peak_hbm()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": ncu_traffic_per_launch(), "peak_source": peak_kind,
-                "kernel": "k_ingest (sketch update)", "alg_bytes_per_launch": alg_per_launch,
+                "kernel": "k_ingest_packed (sketch update)", "alg_bytes_per_launch": alg_per_launch,
                 "avg_launch_ms": ingest_ms_avg, "path_frac": value / world * (alg_step / U) / 1e9 / peak}
     split = {"ingest_ms_per_step": prof["ingest_ms"] / args.steps, "bucket_ms_per_step": prof["bucket_ms"] / args.steps,
              "query_ms_per_step": prof["query_ms"] / args.steps}

@@ -9,15 +9,18 @@
 //                                    then written as coalesced runs
 //   3. k_vert_count, k_scan_*        per-vertex record counts and work chunks ceil(count / chunk)
 //   4. k_vert_scatter                neighbours placed by vertex inside each chunk of a bucket
-//   5. k_ingest                      one warp per work chunk of one vertex.  Lane c owns sketch
-//                                    column c: per record it hashes the edge for its column (XXH3
-//                                    with the column constant folded, gs_common.cuh) and XORs
-//                                    {mix(edge), checksum} into its own shared-memory row for that
-//                                    depth (depths < 10); deeper buckets (probability 2^-10) go
-//                                    straight to HBM with red.global.xor.  At the end of the chunk
-//                                    the non-zero rows and the deterministic bucket are merged into
-//                                    the vertex sketch (plain read-modify-write when the vertex is
-//                                    one chunk, atomic XOR when several warps share it).
+//   5. k_ingest_packed / k_ingest    one warp per work chunk of one vertex.  A lane hashes the edge
+//                                    for one column (XXH3 with the column constant folded,
+//                                    gs_common.cuh) and XORs {mix(edge), checksum} into its own
+//                                    shared-memory row for that depth (depths < 10); deeper buckets
+//                                    (probability 2^-10) go straight to HBM with red.global.xor.
+//                                    k_ingest_packed (at most 32 columns) gives lanes left over by
+//                                    the columns the columns of a fourth record per three rounds;
+//                                    k_ingest (wider sketches, register depths) keeps lane = column.
+//                                    At the end of the chunk the non-zero rows and the deterministic
+//                                    bucket are merged into the vertex sketch (plain read-modify-
+//                                    write when the vertex is one chunk, atomic XOR when several
+//                                    warps share it).
 //
 // XOR is commutative and associative, so the result is bit-identical to the reference's
 // sequential Sketch::update over the same records (src/sketch.cpp:85-99), whatever the order.
@@ -807,6 +810,8 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
     }
 
     const uint32_t zw = kRows * (p1 + (se ? J * 8u : 0u));
+    // every lane main or spare and every spare round with a column (C = 24): no per-round lane test
+    const bool all_live = C + se == 32u && J * se == C;
     for (uint32_t i = lane; i < zw; i += 32) wbase[i] = make_uint4(0, 0, 0, 0);
     uint64_t det_m = 0, det_g = 0;
     __syncwarp();
@@ -842,10 +847,13 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
     };
     auto emix = [](const uint4& q) { return ((uint64_t)q.y << 32) | q.x; };
 
+    // each batch's neighbour ids are loaded one batch ahead, so the load overlaps the previous rounds
+    uint32_t nxt = rb + lane < re ? A.nbr[rb + lane] : 0u;
     for (uint32_t b = rb; b < re; b += 32) {
       const uint32_t r = b + lane;
       const bool valid = r < re;
-      const uint32_t u = valid ? A.nbr[r] - vb : v;
+      const uint32_t u = valid ? nxt - vb : v;
+      if (r + 32 < re) nxt = A.nbr[r + 32];
       const uint64_t E = gs_key_mix(gs_concat(v, u));
       const uint64_t cs = gs_hash_tail(E ^ csmix);
       if (valid) { det_m ^= E; det_g ^= cs; }
@@ -856,7 +864,20 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
       uint32_t k = 0;
       // groups of four records; a0..a2: this lane's record of each round
       uint32_t a0 = rs + ro[0] * 16u, a1 = rs + ro[1] * 16u, a2 = rs + ro[2] * 16u;
-      for (uint32_t gi = 0; gi < ng; gi++, k += J + 1, a0 += 16u * (J + 1), a1 += 16u * (J + 1), a2 += 16u * (J + 1)) {
+      uint32_t gi = 0;
+      if (all_live) {
+        for (; gi < ng; gi++, k += J + 1, a0 += 16u * (J + 1), a1 += 16u * (J + 1), a2 += 16u * (J + 1)) {
+          const uint4 q0 = lds(a0), q1 = lds(a1), q2 = lds(a2);
+          uint32_t h0, h1, h2;
+          const uint32_t d0 = gs_depth_low(emix(q0) ^ cm[0], &h0);
+          const uint32_t d1 = gs_depth_low(emix(q1) ^ cm[1], &h1);
+          const uint32_t d2 = gs_depth_low(emix(q2) ^ cm[2], &h2);
+          update(true, sb[0], col[0], d0, h0, q0);
+          update(true, sb[1], col[1], d1, h1, q1);
+          update(true, sb[2], col[2], d2, h2, q2);
+        }
+      }
+      for (; gi < ng; gi++, k += J + 1, a0 += 16u * (J + 1), a1 += 16u * (J + 1), a2 += 16u * (J + 1)) {
         const uint4 q0 = lds(a0), q1 = lds(a1), q2 = lds(a2);
         uint32_t h0, h1, h2;
         const uint32_t d0 = gs_depth_low(emix(q0) ^ cm[0], &h0);
