@@ -230,6 +230,11 @@ size_t part_scatter_staged_smem(uint32_t H) {
   return (size_t)((4 * H + 1 + 1) & ~1u) * sizeof(uint32_t) + (size_t)2 * kPartEdges * sizeof(uint2);
 }
 
+//
+// COMPACT: the records leave as one word, (key & (2^lb - 1)) << (32 - lb) | neighbour, which holds
+// both whenever every neighbour id is below 2^(32 - lb) (V = 2^17: 9 + 17 bits); pass 2 then reads
+// 4 bytes per record instead of 8.
+template <bool COMPACT>
 __global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint2* __restrict__ pairs, uint64_t n,
                                                                       PairTag t, uint32_t lb, uint32_t H,
                                                                       uint32_t* __restrict__ bkt,
@@ -296,9 +301,17 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint
     const uint2 r = stage[i];
     const uint32_t b = r.x >> lb;
     const uint64_t pos = (uint64_t)gbase[b] + (i - loff[b]);
-    if (pos < cap) part[pos] = r;
-    else atomicOr(status, (uint32_t)GS_DEV_ERR_CAPACITY);
+    if (pos >= cap) atomicOr(status, (uint32_t)GS_DEV_ERR_CAPACITY);
+    else if (COMPACT) reinterpret_cast<uint32_t*>(part)[pos] = ((r.x & ((1u << lb) - 1u)) << (32u - lb)) | r.y;
+    else part[pos] = r;
   }
+}
+
+// key within its bucket of pass-1 record i, in either record form
+template <bool COMPACT>
+__device__ __forceinline__ uint32_t part_key(const uint2* part, uint64_t i, uint32_t lb) {
+  if (COMPACT) return reinterpret_cast<const uint32_t*>(part)[i] >> (32u - lb);
+  return part[i].x & ((1u << lb) - 1u);
 }
 
 // the bucket of pass-2 chunk c: largest d with choff[d] <= c
@@ -312,6 +325,7 @@ __device__ __forceinline__ uint32_t chunk_bucket(const uint32_t* choff, uint32_t
 }
 
 // pass 2, counting: records per vertex of each bucket chunk
+template <bool COMPACT>
 __global__ void __launch_bounds__(kPartThreads) k_vert_count(const uint2* __restrict__ part, const uint32_t* __restrict__ bkt,
                                                              uint32_t H, uint32_t lb, uint32_t* __restrict__ cnt,
                                                              const uint32_t* __restrict__ status) {
@@ -328,7 +342,7 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_count(const uint2* __rest
     const uint32_t d = s_d;
     const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
     const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
-    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&hist[part[i].x & mask], 1u);
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&hist[part_key<COMPACT>(part, i, lb)], 1u);
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < nk; k += blockDim.x)
       if (hist[k]) atomicAdd(&cnt[(d << lb) + k], hist[k]);
@@ -337,6 +351,7 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_count(const uint2* __rest
 }
 
 // pass 2, placement: each record's neighbour goes to its vertex's slice of nbr
+template <bool COMPACT>
 __global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __restrict__ part, const uint32_t* __restrict__ bkt,
                                                                uint32_t H, uint32_t lb, uint32_t* __restrict__ cursor,
                                                                uint32_t* __restrict__ nbr, uint64_t cap,
@@ -356,7 +371,7 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __re
     const uint32_t d = s_d;
     const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
     const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
-    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&hist[part[i].x & mask], 1u);
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&hist[part_key<COMPACT>(part, i, lb)], 1u);
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < nk; k += blockDim.x) {
       const uint32_t h = hist[k];
@@ -365,10 +380,18 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __re
     }
     __syncthreads();
     for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      const uint2 r = part[i];
-      const uint32_t k = r.x & mask;
+      uint32_t k, u;
+      if (COMPACT) {
+        const uint32_t r = reinterpret_cast<const uint32_t*>(part)[i];
+        k = r >> (32u - lb);
+        u = r & ((1u << (32u - lb)) - 1u);
+      } else {
+        const uint2 r = part[i];
+        k = r.x & mask;
+        u = r.y;
+      }
       const uint32_t pos = base[k] + atomicAdd(&hist[k], 1u);
-      if (pos < cap) nbr[pos] = r.y;
+      if (pos < cap) nbr[pos] = u;
       else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
     }
     __syncthreads();
@@ -1024,6 +1047,7 @@ gs_status launch_ingest_s(gs_graph* g, uint32_t nv, bool small, cudaStream_t s) 
   return small ? launch_ingest_r<CG, true, TEN>(g, nv, s) : launch_ingest_r<CG, false, TEN>(g, nv, s);
 }
 
+template <bool COMPACT>
 gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& t, uint32_t lb, uint32_t H,
                                      uint32_t* bkt, uint2* part, uint64_t cap, uint32_t* status, cudaStream_t s) {
   const size_t smem = part_scatter_staged_smem(H);
@@ -1031,11 +1055,11 @@ gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& 
   int dev = 0;
   GS_CUDA_TRY(cudaGetDevice(&dev));
   if (smem_set[dev & 63] < smem) {
-    GS_CUDA_TRY(cudaFuncSetAttribute(k_part_scatter_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_part_scatter_staged<COMPACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     smem_set[dev & 63] = smem;
   }
   const unsigned tiles = (unsigned)((m + kPartEdges - 1) / kPartEdges);
-  k_part_scatter_staged<<<tiles, kPartThreads, smem, s>>>(p, m, t, lb, H, bkt, part, cap, status);
+  k_part_scatter_staged<COMPACT><<<tiles, kPartThreads, smem, s>>>(p, m, t, lb, H, bkt, part, cap, status);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
 }
@@ -1151,17 +1175,28 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
     }
     {
       GsProfScope ps(g, GS_PROF_BUCKET, s, 6);
+      // one-word records when a bucket-local key and a neighbour id fit together
+      const bool compact = !tagged && (uint64_t)g->V <= (1ull << (32u - lb));
       if (tagged) {
         k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, m, t, lb, H, g->d_bkt, g->d_part,
                                                                              g->part_cap, g->d_status);
+      } else if (compact) {
+        GS_TRY(launch_part_scatter_staged<true>(p, m, t, lb, H, g->d_bkt, g->d_part, g->part_cap, g->d_status, s));
       } else {
-        GS_TRY(launch_part_scatter_staged(p, m, t, lb, H, g->d_bkt, g->d_part, g->part_cap, g->d_status, s));
+        GS_TRY(launch_part_scatter_staged<false>(p, m, t, lb, H, g->d_bkt, g->d_part, g->part_cap, g->d_status, s));
       }
-      k_vert_count<<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt,
-                                                                             g->d_status);
-      GS_TRY(scan_counts(g, nv, s));
-      k_vert_scatter<<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(
-          g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status);
+      const size_t vc_smem = (1u << lb) * sizeof(uint32_t), vs_smem = 2 * (1u << lb) * sizeof(uint32_t);
+      if (compact) {
+        k_vert_count<true><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status);
+        GS_TRY(scan_counts(g, nv, s));
+        k_vert_scatter<true><<<grid2, kPartThreads, vs_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr,
+                                                                  g->nbr_cap, g->d_status);
+      } else {
+        k_vert_count<false><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status);
+        GS_TRY(scan_counts(g, nv, s));
+        k_vert_scatter<false><<<grid2, kPartThreads, vs_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr,
+                                                                   g->nbr_cap, g->d_status);
+      }
       GS_CUDA_TRY(cudaGetLastError());
     }
     {
@@ -1252,12 +1287,12 @@ gs_status gs_ingest_pairs_on_scratch(const GsScratchIngest& x, cudaStream_t s) {
   k_part_scan<<<1, kScanThreads, 0, s>>>(x.bkt, H, x.status);
   k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, x.n, t, lb, H, x.bkt, x.part,
                                                                        x.records_cap, x.status);
-  k_vert_count<<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.status);
+  k_vert_count<false><<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.status);
   const uint32_t stiles = (nv + kScanTile - 1) / kScanTile;
   k_scan_tiles<<<stiles, kScanThreads, 0, s>>>(x.cnt, nv, x.chunk, x.off, x.choff, x.tile);
   k_scan_top<<<1, kScanThreads, 0, s>>>(x.tile, stiles, x.off, x.choff, nv, x.status);
   k_scan_add<<<stiles, kScanThreads, 0, s>>>(x.off, x.choff, x.cnt, x.tile, nv);
-  k_vert_scatter<<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.nbr,
+  k_vert_scatter<false><<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.nbr,
                                                                                 x.records_cap, x.status);
   GS_CUDA_TRY(cudaGetLastError());
   const bool small = x.geom.bkt_per_col < (uint32_t)kSlabDepth;
