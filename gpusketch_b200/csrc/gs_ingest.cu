@@ -119,6 +119,7 @@ constexpr int kPartThreads = 512;
 constexpr int kPartEdges = 4096;      // edges per block in pass 1
 constexpr int kVertChunk = 8192;      // partitioned records per block iteration in pass 2
 constexpr int kMaxBuckets = 4096;
+constexpr int kVertUnroll = 8;        // records a pass-2 thread loads before its shared-memory atomics
 
 __global__ void __launch_bounds__(kPartThreads) k_part_count(const uint2* __restrict__ pairs, uint64_t n, PairTag t,
                                                              uint32_t lb, uint32_t H, uint32_t* __restrict__ tot,
@@ -128,13 +129,24 @@ __global__ void __launch_bounds__(kPartThreads) k_part_count(const uint2* __rest
   __syncthreads();
   const uint64_t e0 = (uint64_t)blockIdx.x * kPartEdges;
   const uint64_t e1 = min(n, e0 + kPartEdges);
-  for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-    const uint2 p = pairs[e];
-    int lo = 0, hi = -1;
-    if (!record_levels(t, p.x, p.y, &lo, &hi, status)) continue;
-    for (int g = lo; g <= hi; g++) {
-      atomicAdd(&hist[((uint32_t)g * t.V + p.x) >> lb], 1u);
-      atomicAdd(&hist[((uint32_t)g * t.V + p.y) >> lb], 1u);
+  for (uint64_t b = e0; b < e1; b += (uint64_t)blockDim.x * kVertUnroll) {
+    uint2 ps[kVertUnroll];
+#pragma unroll
+    for (int j = 0; j < kVertUnroll; j++) {
+      const uint64_t e = b + threadIdx.x + (uint64_t)j * blockDim.x;
+      ps[j] = e < e1 ? pairs[e] : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int j = 0; j < kVertUnroll; j++) {
+      const uint64_t e = b + threadIdx.x + (uint64_t)j * blockDim.x;
+      if (e >= e1) continue;
+      const uint2 p = ps[j];
+      int lo = 0, hi = -1;
+      if (!record_levels(t, p.x, p.y, &lo, &hi, status)) continue;
+      for (int g = lo; g <= hi; g++) {
+        atomicAdd(&hist[((uint32_t)g * t.V + p.x) >> lb], 1u);
+        atomicAdd(&hist[((uint32_t)g * t.V + p.y) >> lb], 1u);
+      }
     }
   }
   __syncthreads();
@@ -342,7 +354,17 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_count(const uint2* __rest
     const uint32_t d = s_d;
     const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
     const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
-    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&hist[part_key<COMPACT>(part, i, lb)], 1u);
+    for (uint32_t b = r0; b < r1; b += blockDim.x * kVertUnroll) {
+      uint32_t ks[kVertUnroll];
+#pragma unroll
+      for (int j = 0; j < kVertUnroll; j++) {
+        const uint32_t i = b + threadIdx.x + j * blockDim.x;
+        ks[j] = i < r1 ? part_key<COMPACT>(part, i, lb) : 0xffffffffu;
+      }
+#pragma unroll
+      for (int j = 0; j < kVertUnroll; j++)
+        if (ks[j] != 0xffffffffu) atomicAdd(&hist[ks[j]], 1u);
+    }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < nk; k += blockDim.x)
       if (hist[k]) atomicAdd(&cnt[(d << lb) + k], hist[k]);
@@ -371,7 +393,17 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __re
     const uint32_t d = s_d;
     const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
     const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
-    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) atomicAdd(&hist[part_key<COMPACT>(part, i, lb)], 1u);
+    for (uint32_t b = r0; b < r1; b += blockDim.x * kVertUnroll) {
+      uint32_t ks[kVertUnroll];
+#pragma unroll
+      for (int j = 0; j < kVertUnroll; j++) {
+        const uint32_t i = b + threadIdx.x + j * blockDim.x;
+        ks[j] = i < r1 ? part_key<COMPACT>(part, i, lb) : 0xffffffffu;
+      }
+#pragma unroll
+      for (int j = 0; j < kVertUnroll; j++)
+        if (ks[j] != 0xffffffffu) atomicAdd(&hist[ks[j]], 1u);
+    }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < nk; k += blockDim.x) {
       const uint32_t h = hist[k];
@@ -379,20 +411,32 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __re
       hist[k] = 0;
     }
     __syncthreads();
-    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      uint32_t k, u;
-      if (COMPACT) {
-        const uint32_t r = reinterpret_cast<const uint32_t*>(part)[i];
-        k = r >> (32u - lb);
-        u = r & ((1u << (32u - lb)) - 1u);
-      } else {
-        const uint2 r = part[i];
-        k = r.x & mask;
-        u = r.y;
+    for (uint32_t b = r0; b < r1; b += blockDim.x * kVertUnroll) {
+      uint32_t ks[kVertUnroll], us[kVertUnroll];
+#pragma unroll
+      for (int j = 0; j < kVertUnroll; j++) {
+        const uint32_t i = b + threadIdx.x + j * blockDim.x;
+        ks[j] = 0xffffffffu;
+        us[j] = 0;
+        if (i < r1) {
+          if (COMPACT) {
+            const uint32_t r = reinterpret_cast<const uint32_t*>(part)[i];
+            ks[j] = r >> (32u - lb);
+            us[j] = r & ((1u << (32u - lb)) - 1u);
+          } else {
+            const uint2 r = part[i];
+            ks[j] = r.x & mask;
+            us[j] = r.y;
+          }
+        }
       }
-      const uint32_t pos = base[k] + atomicAdd(&hist[k], 1u);
-      if (pos < cap) nbr[pos] = u;
-      else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
+#pragma unroll
+      for (int j = 0; j < kVertUnroll; j++) {
+        if (ks[j] == 0xffffffffu) continue;
+        const uint32_t pos = base[ks[j]] + atomicAdd(&hist[ks[j]], 1u);
+        if (pos < cap) nbr[pos] = us[j];
+        else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
+      }
     }
     __syncthreads();
   }
