@@ -77,7 +77,10 @@ gs_status order_after(gs_graph* g, cudaStream_t s) {
   return GS_OK;
 }
 
-uint64_t staging_pairs(const gs_graph* g) { return std::min<uint64_t>(g->max_batch_edges, 1ull << 25); }
+// Host input moves in slices of at most 2^24 pairs.  Per phase the first copy and the last slice's
+// ingest overlap nothing and every slice carries a fixed ingest cost (about 0.5 ms at V = 2^17);
+// 2^24 balances the two (1 GiB phases: 202.6 ms per 8 phases at 2^25, 189.1 at 2^24, 211.9 at 2^23).
+uint64_t staging_pairs(const gs_graph* g) { return std::min<uint64_t>(g->max_batch_edges, 1ull << 24); }
 
 }  // namespace
 
