@@ -66,6 +66,18 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def ncu_issue_per_launch():
+    """warp instructions of one full-size ingest launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "k_ingest_rmat17_issue.txt")
+    try:
+        for line in open(path):
+            if line.startswith("warp_instructions_per_full_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
 def ncu_traffic_per_launch():
     """dram bytes read+write of one full-size ingest launch from the committed ncu summary, or None."""
     path = os.path.join(ROOT, "profiles", "k_ingest_rmat17_traffic.txt")
@@ -456,6 +468,17 @@ def run_gs(args):
                 "traffic": ncu_traffic_per_launch(), "peak_source": peak_kind,
                 "kernel": "k_ingest_packed (sketch update)", "alg_bytes_per_launch": alg_per_launch,
                 "avg_launch_ms": ingest_ms_avg, "path_frac": value / world * (alg_step / U) / 1e9 / peak}
+    # the sketch update is bound by instruction issue: its measured warp instructions per launch
+    # (one-pass ncu count of this workload's launch) against 4 schedulers x SMs x the sampled SM clock
+    issue = None
+    inst = ncu_issue_per_launch()
+    if inst is not None and V == (1 << 17) and phase == (1 << 27) and clocks.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        ach = inst / (ingest_ms_avg / 1e3)
+        pk = 4.0 * sms * clocks["sm_mhz"] * 1e6
+        issue = {"bound": "issue", "achieved": ach, "peak": pk, "unit": "warp_inst/s", "frac": ach / pk,
+                 "inst_per_launch": inst, "kernel": "k_ingest_packed (sketch update)",
+                 "peak_source": f"4 schedulers x {sms} SMs x median sampled SM clock"}
     split = {"ingest_ms_per_step": prof["ingest_ms"] / args.steps, "bucket_ms_per_step": prof["bucket_ms"] / args.steps,
              "query_ms_per_step": prof["query_ms"] / args.steps}
 
@@ -516,7 +539,8 @@ def run_gs(args):
                    "stream_seed": f"{STREAM_SEED:#x}+rank", "sketch_seed": f"{SKETCH_SEED:#x}+rank",
                    "sketch_bytes_per_vertex": Sv, "l2": "inputs larger than L2 (8 GiB of records per GPU)",
                    "parallelism": f"replicas x{world}", "tuning": tuning},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": prof["kernel_launches"],
+        "roofline": roofline, "issue_roofline": issue, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": prof["kernel_launches"],
         "clocks": clocks, "kernel_split": split, "batched": batched, "served": served,
         "mincut": mincut,
     }
