@@ -520,6 +520,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_top(uint32_t* __restrict_
     choff[nv] = carry.y;
     status[1] = carry.x;
     status[2] = carry.y;
+    status[14] = 0;  // next work chunk of the packed sketch update
   }
 }
 
@@ -555,6 +556,7 @@ struct IngestArgs {
   const uint32_t* vtenant;       // tenant of every vertex (tenant variant only)
   const GsIngTenant* tenants;    // geometry and arena offset of every tenant (tenant variant only)
   uint32_t warp_words;           // shared memory per warp in uint4 (packed variant only)
+  uint32_t* next_chunk;          // work-chunk counter, zero at launch (packed variant only)
 };
 
 // ---- packed lane layout (sketches of at most 24 columns) ----
@@ -848,10 +850,12 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
   if (!TEN) set_geometry(A.C, A.colmix);
 
   const uint32_t total = A.status[2];
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-
-  for (uint32_t ch = gw; ch < total; ch += nw) {
+  // warps take work chunks from a counter, so no warp idles while others still have long chunks
+  // left; lane 0 fetches the next index while the current chunk runs
+  uint32_t nxt = 0;
+  if (lane == 0) nxt = atomicAdd(A.next_chunk, 1u);
+  for (uint32_t ch = __shfl_sync(0xffffffffu, nxt, 0); ch < total; ch = __shfl_sync(0xffffffffu, nxt, 0)) {
+    if (lane == 0) nxt = atomicAdd(A.next_chunk, 1u);
     const uint32_t vv = chunk_owner(A, ch, lane);
     const uint32_t c0ff = A.choff[vv];
     const bool exclusive = (A.choff[vv + 1] - c0ff) == 1;
@@ -1016,6 +1020,7 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   A.status = g->d_status; A.nv = nv; A.V = g->V; A.C = g->geom.num_columns;
   A.bkt = g->geom.bkt_per_col; A.nb = g->geom.num_buckets; A.chunk = g->tune.chunk;
   A.warp_words = 0;
+  A.next_chunk = nullptr;
   const int warps = (int)g->tune.warps_per_block;
   const size_t smem = ingest_smem_bytes(CG, R, warps);
   // the opt-in shared-memory limit is a per-device function attribute; the persistent grid fills
@@ -1056,6 +1061,7 @@ gs_status launch_ingest_packed(gs_graph* g, uint32_t nv, cudaStream_t s) {
   A.vtenant = TEN ? g->d_vtenant : nullptr;
   A.tenants = TEN ? g->d_ten : nullptr;
   A.warp_words = packed_warp_words(g);
+  A.next_chunk = g->d_status + 14;
   const int warps = std::min(kPackMaxThreads / 32, (int)g->tune.warps_per_block);
   const size_t smem = (size_t)warps * A.warp_words * sizeof(uint4);
   struct Cache { size_t smem = 0; int warps = 0; int blocks = 0; };
@@ -1304,6 +1310,7 @@ gs_status launch_ingest_scratch(const GsScratchIngest& x, cudaStream_t s) {
   A.vtenant = nullptr;
   A.tenants = nullptr;
   A.warp_words = 0;
+  A.next_chunk = nullptr;
   const size_t smem = ingest_smem_bytes(CG, 1, (int)x.warps);
   int nb = 0;
   GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, 1, SMALL, false>, (int)x.warps * 32, smem));
