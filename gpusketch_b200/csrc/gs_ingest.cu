@@ -672,7 +672,14 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
 
-  for (uint32_t ch = gw; ch < total; ch += nw) {
+  // with a chunk counter, warps take work chunks from it (lane 0 fetches the next index while the
+  // current chunk runs); without one, a fixed stride
+  const bool dyn = A.next_chunk != nullptr;
+  uint32_t nxt = 0;
+  if (dyn && lane == 0) nxt = atomicAdd(A.next_chunk, 1u);
+  for (uint32_t ch = dyn ? __shfl_sync(0xffffffffu, nxt, 0) : gw; ch < total;
+       ch = dyn ? __shfl_sync(0xffffffffu, nxt, 0) : ch + nw) {
+    if (dyn && lane == 0) nxt = atomicAdd(A.next_chunk, 1u);
     const uint32_t vv = chunk_owner(A, ch, lane);
     const uint32_t c0 = A.choff[vv];
     const bool exclusive = (A.choff[vv + 1] - c0) == 1;
@@ -1020,7 +1027,7 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   A.status = g->d_status; A.nv = nv; A.V = g->V; A.C = g->geom.num_columns;
   A.bkt = g->geom.bkt_per_col; A.nb = g->geom.num_buckets; A.chunk = g->tune.chunk;
   A.warp_words = 0;
-  A.next_chunk = nullptr;
+  A.next_chunk = g->d_status + 14;
   const int warps = (int)g->tune.warps_per_block;
   const size_t smem = ingest_smem_bytes(CG, R, warps);
   // the opt-in shared-memory limit is a per-device function attribute; the persistent grid fills
