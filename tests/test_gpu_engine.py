@@ -84,6 +84,27 @@ def test_tenants_match_solo_runs(restatement, device_input):
             assert e.download(t).tobytes() == sk.tobytes()
 
 
+def test_large_vertex_space_two_word_records(restatement):
+    """In a 2^22-id vertex space a bucket-local key (11 bits) and a neighbour id (22 bits) do not fit one
+    32-bit word, so the bucketing passes move (key, neighbour) pairs; the tenants' sketches and answers
+    still equal solo runs."""
+    rng = np.random.default_rng(12)
+    with make_engine(max_vertices=1 << 22) as e:
+        specs = TENANTS[:3]
+        ids, streams = [], []
+        for V, seed, f, gen in specs:
+            t = e.add_tenant(V, seed, f)
+            ids.append(t)
+            streams.append((t, gen()))
+        tens, offs, pairs = interleaved_slices(streams, 2, rng)
+        e.ingest(tens, offs, pairs)
+        res = e.connected_components(ids)
+        for (V, seed, f, _), (t, a) in zip(specs, streams):
+            sk, labels, ncc, rounds = solo(V, seed, f, a)
+            assert e.download(t).tobytes() == sk, t
+            assert np.array_equal(res[t].labels, labels), t
+
+
 def test_query_subsets_and_repeated_queries():
     rng = np.random.default_rng(8)
     with make_engine() as e:
