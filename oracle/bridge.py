@@ -11,6 +11,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libgsoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgsref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libgsrefgpu.so")
 
 _u32 = np.ctypeslib.ndpointer(np.uint32, flags="C")
 _u64 = np.ctypeslib.ndpointer(np.uint64, flags="C")
@@ -285,3 +286,51 @@ class RefMC:
 def parse_header(binary: bytes):
     seed, V, factor = struct.unpack_from("<QId", binary, 0)
     return seed, V, factor
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
+
+
+class RefGpuKernel:
+    """The reference's own GPU sketch-update kernel (src/cuda_kernel.cu:152-257 of the reference, built
+    for sm_100a into oracle/_ref/libgsrefgpu.so by oracle/Makefile).  Device pointers are plain ints."""
+
+    def __init__(self):
+        L = _load(REF_GPU_SO)
+        L.gsref_gpu_prepare.restype = C.c_int
+        L.gsref_gpu_prepare.argtypes = [C.c_uint64]
+        L.gsref_gpu_sketch_update.restype = C.c_int
+        L.gsref_gpu_sketch_update.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                                              C.c_uint64, C.c_void_p]
+        self.L = L
+
+    def prepare(self, num_buckets: int) -> None:
+        assert self.L.gsref_gpu_prepare(num_buckets) == 0
+
+    def sketch_update(self, num_threads, num_batches, stream, d_dsts, d_src, d_sizes, d_start, geo, seed, d_deltas):
+        rc = self.L.gsref_gpu_sketch_update(num_threads, num_batches, stream, d_dsts, d_src, d_sizes, d_start,
+                                            geo["num_samples"], geo["num_buckets"], geo["num_columns"],
+                                            geo["bkt_per_col"], seed, d_deltas)
+        assert rc == 0, rc
+
+
+def ref_batches(pairs: np.ndarray, batch_size: int):
+    """The reference's per-vertex batch form of an edge-record stream (GraphSketchDriver gutters ->
+    apply_update_batch): both directions of every non-self-loop record, grouped by source vertex,
+    each vertex's destinations cut into batches of at most batch_size.  Returns
+    (dsts u32, batch src u32, batch start u64, batch size u64)."""
+    p = np.asarray(pairs, np.uint32).reshape(-1, 2)
+    p = p[p[:, 0] != p[:, 1]]
+    src = np.concatenate([p[:, 0], p[:, 1]])
+    dst = np.concatenate([p[:, 1], p[:, 0]])
+    order = np.argsort(src, kind="stable")
+    src, dst = src[order], dst[order]
+    uniq, first, counts = np.unique(src, return_index=True, return_counts=True)
+    nb = (counts + batch_size - 1) // batch_size
+    j = np.arange(int(nb.sum())) - np.repeat(np.cumsum(nb) - nb, nb)
+    bsrc = np.repeat(uniq, nb).astype(np.uint32)
+    bstart = (np.repeat(first, nb) + j * batch_size).astype(np.uint64)
+    bsize = np.minimum(batch_size, np.repeat(counts, nb) - j * batch_size).astype(np.uint64)
+    return np.ascontiguousarray(dst, np.uint32), bsrc, bstart, bsize
