@@ -112,6 +112,21 @@ def test_hub_vertex_spans_many_chunks(restatement):
     assert ncc == n and np.array_equal(labels, exact)
 
 
+@pytest.mark.parametrize("factor", [1.38, 1.45, 1.5, 1.6, 1.66, 1.75, 1.8, 1.9, 1.95, 2.0, 2.1, 2.2, 2.25, 2.3, 2.4])
+def test_every_column_count_of_the_packed_layout(restatement, factor):
+    """V=1024 with sketches_factor 1.38 .. 2.4 gives 19 .. 33 columns: spare lanes with and without an
+    idle lane or a spare round without a column (19..23), every lane busy (24), no spare lanes
+    (25..32), two columns per lane (33).  A hub vertex spans several work chunks."""
+    V, seed = 1024, 0x5EED3000
+    rng = np.random.default_rng(int(factor * 100))
+    pairs = rng.integers(0, V, size=(20000, 2), dtype=np.uint32)
+    hub = np.stack([np.full(3000, 7, np.uint32), rng.integers(0, V, 3000, dtype=np.uint32)], axis=1)
+    pairs = np.concatenate([pairs, hub])
+    with gs.GraphSketch(V, seed, sketches_factor=factor) as g:
+        g.ingest_pairs(pairs)
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs, factor), g.geometry.num_columns
+
+
 def test_more_than_32_columns(restatement):
     """sketches_factor 3 at V=4096 gives 49 columns: two columns per lane."""
     V, seed, f = 4096, 5, 3.0
