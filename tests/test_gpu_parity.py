@@ -127,6 +127,23 @@ def test_every_column_count_of_the_packed_layout(restatement, factor):
         assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs, factor), g.geometry.num_columns
 
 
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_input_across_many_staging_slices(restatement, pinned):
+    """Host records larger than the staging ring move in slices through both pinned/device slots: pageable
+    input is copied into the library's pinned ring, page-locked input is copied from in place.  The
+    sketches equal the oracle's."""
+    import torch
+    V, seed = 4096, 0x5EED3100
+    rng = np.random.default_rng(31)
+    pairs = rng.integers(0, V, size=(200_003, 2), dtype=np.uint32)
+    src = torch.from_numpy(pairs.view(np.int32)).pin_memory() if pinned else pairs
+    with gs.GraphSketch(V, seed, max_batch_edges=1 << 14) as g:
+        g.ingest_pairs(src)
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs)
+        labels, _, _ = g.connected_components()
+    assert np.array_equal(labels, restatement.exact_cc(V, pairs)[1])
+
+
 def test_more_than_32_columns(restatement):
     """sketches_factor 3 at V=4096 gives 49 columns: two columns per lane."""
     V, seed, f = 4096, 5, 3.0
