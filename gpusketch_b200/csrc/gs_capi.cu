@@ -80,6 +80,13 @@ gs_status order_after(gs_graph* g, cudaStream_t s) {
 // Host input moves in slices of at most 2^24 pairs.  Per phase the first copy and the last slice's
 // ingest overlap nothing and every slice carries a fixed ingest cost (about 0.5 ms at V = 2^17);
 // 2^24 balances the two (1 GiB phases: 202.6 ms per 8 phases at 2^25, 189.1 at 2^24, 211.9 at 2^23).
+// (src[i], dst[i]) -> pair i
+__global__ void k_interleave(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint2* __restrict__ out,
+                             uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = make_uint2(a[i], b[i]);
+}
+
 uint64_t staging_pairs(const gs_graph* g) { return std::min<uint64_t>(g->max_batch_edges, 1ull << 24); }
 
 }  // namespace
@@ -255,18 +262,30 @@ gs_status gs_ingest_edges(gs_graph* g, const uint32_t* src, const uint32_t* dst,
   if (!g || (n && (!src || !dst))) { gs_set_error("gs_ingest_edges: null argument"); return GS_ERR_BAD_ARG; }
   if (n == 0) return GS_OK;
   GS_GUARD(g);
-  std::vector<uint32_t> host;
-  if (on_device) {
-    host.resize(2 * n);
-    std::vector<uint32_t> a(n), b(n);
-    GS_CUDA_TRY(cudaMemcpy(a.data(), src, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    GS_CUDA_TRY(cudaMemcpy(b.data(), dst, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    for (uint64_t i = 0; i < n; i++) { host[2 * i] = a[i]; host[2 * i + 1] = b[i]; }
-  } else {
-    host.resize(2 * n);
+  if (!on_device) {
+    std::vector<uint32_t> host(2 * n);
     for (uint64_t i = 0; i < n; i++) { host[2 * i] = src[i]; host[2 * i + 1] = dst[i]; }
+    return gs_ingest_pairs(g, host.data(), n, 0, stream);
   }
-  return gs_ingest_pairs(g, host.data(), n, 0, stream);
+  // device arrays: interleaved on the device into the staging slots, one slice at a time
+  cudaStream_t s = pick_stream(g, stream);
+  g->labels_valid = false;
+  GS_TRY(gs_ensure_pair_staging(g));
+  const uint64_t cap = g->pairs_cap;
+  for (uint64_t done = 0, k = 0; done < n; k++) {
+    const uint64_t m = std::min(cap, n - done);
+    const int slot = (int)(k & 1);
+    uint32_t* dslot = g->d_pairs + (size_t)slot * cap * 2;
+    // the slot's previous slice must be consumed before it is overwritten
+    GS_CUDA_TRY(cudaStreamWaitEvent(s, g->ev_done[slot], 0));
+    const int grid = (int)std::min<uint64_t>((m + 255) / 256, (uint64_t)g->num_sms * 8);
+    k_interleave<<<grid, 256, 0, s>>>(src + done, dst + done, reinterpret_cast<uint2*>(dslot), m);
+    GS_CUDA_TRY(cudaGetLastError());
+    GS_TRY(gs_ingest_device_pairs(g, dslot, m, -1, s));
+    GS_CUDA_TRY(cudaEventRecord(g->ev_done[slot], s));
+    done += m;
+  }
+  return order_after(g, s);
 }
 
 gs_status gs_ingest_vertex_batches(gs_graph* g, uint32_t level, const uint32_t* srcs, const uint64_t* starts,

@@ -58,6 +58,21 @@ def _as_pairs(pairs):
     return C.c_void_p(a.ctypes.data), a.size // 2, False, a
 
 
+def _as_u32(values):
+    """(pointer, count, on_device, keepalive) for a 1-D uint32 array or 32-bit tensor."""
+    try:
+        import torch
+        if isinstance(values, torch.Tensor):
+            if values.dtype not in (torch.int32, torch.uint32):
+                raise TypeError("vertex ids must be 32-bit integers")
+            t = values.contiguous()
+            return C.c_void_p(t.data_ptr()), t.numel(), bool(t.is_cuda), t
+    except ImportError:  # pragma: no cover
+        pass
+    a = np.ascontiguousarray(values, dtype=np.uint32)
+    return C.c_void_p(a.ctypes.data), a.size, False, a
+
+
 def _stream_ptr(stream) -> C.c_void_p:
     if stream is None:
         return C.c_void_p(0)
@@ -117,6 +132,16 @@ class GraphSketch:
         p, n, dev, keep = _as_pairs(pairs)
         check(self._lib.gs_ingest_pairs(self._h, p, n, int(dev), _stream_ptr(stream)), "gs_ingest_pairs")
         del keep
+
+    def ingest_edges(self, src, dst, stream=None) -> None:
+        """gs_ingest_edges: record i toggles edge {src[i], dst[i]}; both arrays on the host or both on
+        the device."""
+        a, na, da, ka = _as_u32(src)
+        b, nb, db, kb = _as_u32(dst)
+        if na != nb or da != db:
+            raise ValueError("src and dst need the same length and the same side (host or device)")
+        check(self._lib.gs_ingest_edges(self._h, a, b, na, int(da), _stream_ptr(stream)), "gs_ingest_edges")
+        del ka, kb
 
     def ingest_vertex_batches(self, srcs, starts, sizes, dsts, level: int = 0) -> None:
         s = np.ascontiguousarray(srcs, dtype=np.uint32)

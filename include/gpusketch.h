@@ -121,7 +121,7 @@ uint64_t gs_desired_updates_per_batch(const gs_graph* g);
 gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int pairs_on_device,
                           void* cuda_stream);
 
-/* Same as gs_ingest_pairs with separate src / dst arrays. */
+/* Same as gs_ingest_pairs with separate src / dst arrays (device arrays are interleaved on the device). */
 gs_status gs_ingest_edges(gs_graph* g, const uint32_t* src, const uint32_t* dst, uint64_t n,
                           int on_device, void* cuda_stream);
 

@@ -144,6 +144,22 @@ def test_host_input_across_many_staging_slices(restatement, pinned):
     assert np.array_equal(labels, restatement.exact_cc(V, pairs)[1])
 
 
+@pytest.mark.parametrize("on_device", [False, True])
+def test_ingest_edges_src_dst_arrays(restatement, on_device):
+    """gs_ingest_edges (separate src / dst arrays, interleaved on the device for device input, in several
+    staging slices) gives the same sketches as the oracle."""
+    import torch
+    V, seed = 2048, 0x5EED3200
+    rng = np.random.default_rng(32)
+    pairs = rng.integers(0, V, size=(70_001, 2), dtype=np.uint32)
+    src, dst = np.ascontiguousarray(pairs[:, 0]), np.ascontiguousarray(pairs[:, 1])
+    if on_device:
+        src, dst = torch.from_numpy(src.view(np.int32)).cuda(), torch.from_numpy(dst.view(np.int32)).cuda()
+    with gs.GraphSketch(V, seed, max_batch_edges=1 << 14) as g:
+        g.ingest_edges(src, dst)
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs)
+
+
 def test_more_than_32_columns(restatement):
     """sketches_factor 3 at V=4096 gives 49 columns: two columns per lane."""
     V, seed, f = 4096, 5, 3.0
