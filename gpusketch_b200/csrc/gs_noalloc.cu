@@ -8,13 +8,14 @@
 // most GS_NOALLOC_MAX_VERTICES vertices and GS_NOALLOC_MAX_EDGES records per call.  Every GPU that
 // loads the library holds that array (about 2.3 MB) until the process exits.
 //
-// In host code the name g_noalloc_scratch is only a host-side stand-in for the array: the device
-// address is obtained with cudaGetSymbolAddress once per device, with that device current, the
-// first time the entry point runs there.  That first call should come before any stream capture.
+// In host code the name g_noalloc_scratch is only a host-side stand-in for the array: every call
+// asks the runtime for the array's device address on the current device (cudaGetSymbolAddress, with
+// that device current) and hands that address to the kernels.  Resolving it per call costs a few
+// microseconds and stays right after cudaDeviceReset, which reloads the module at a new address.
 // All calls share the one array and it keeps the last call's contents, so calls on the same device
-// that overlap on the GPU (different streams, or different host threads) race on it.
-#include <mutex>
-
+// that overlap on the GPU (different streams, or different host threads) race on it.  A call waits
+// for its own stream before it returns (it reads the device error word back), so it cannot be made
+// while that stream is being captured into a CUDA graph.
 #include "gs_internal.h"
 
 namespace {
@@ -41,29 +42,16 @@ constexpr uint64_t kScratchBytes = kOffNbr + al256(kMaxRecords * 4);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-std::mutex g_setup_mtx;
-unsigned char* g_scratch_ptr[64] = {};
-int g_num_sms[64] = {};
-
-// device address of the scratch array on the current device (set up once per device)
+// device address of the scratch array on the current device, and the device's SM count
 gs_status scratch_for_current_device(unsigned char** out, int* sms) {
   int dev = 0;
   GS_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) {
-    gs_set_error("gs_ingest_pairs_noalloc: device ordinal above 63");
-    return GS_ERR_BAD_ARG;
-  }
-  std::lock_guard<std::mutex> lk(g_setup_mtx);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    GS_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    int n = 0;
-    GS_CUDA_TRY(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
-    g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
-    g_num_sms[dev] = n > 0 ? n : 1;
-  }
-  *out = g_scratch_ptr[dev];
-  *sms = g_num_sms[dev];
+  void* p = nullptr;
+  GS_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+  int n = 0;
+  GS_CUDA_TRY(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  *out = static_cast<unsigned char*>(p);
+  *sms = n > 0 ? n : 1;
   return GS_OK;
 }
 
@@ -133,7 +121,8 @@ extern "C" gs_status gs_ingest_pairs_noalloc(uint32_t num_vertices, uint64_t see
   GS_CUDA_TRY(cudaMemcpyAsync(&err, x.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GS_CUDA_TRY(cudaStreamSynchronize(s));
   if (err & GS_DEV_ERR_VERTEX_RANGE) {
-    gs_set_error("gs_ingest_pairs_noalloc: a record named a vertex id >= num_vertices; it was skipped");
+    gs_set_error("gs_ingest_pairs_noalloc: a record named a vertex id >= num_vertices; it was skipped and every "
+                 "other record of the call was applied");
     return GS_ERR_BAD_ARG;
   }
   if (err) {

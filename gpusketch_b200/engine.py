@@ -14,7 +14,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._native import GS_ERR_OOM, GS_PHASE_CUDA_GRAPH, GpuSketchError, GsEngineConfig, GsGeometry, GsProfile, check, lib
-from .graph import BUCKET_DTYPE, Geometry, _as_pairs, _stream_ptr
+from .graph import BUCKET_DTYPE, Geometry, _as_pairs, _device_stream, _stream_ptr
 
 
 def tenant_bytes(num_vertices: int, sketches_factor: float = 1.0) -> int:
@@ -111,7 +111,7 @@ class SketchEngine:
             raise ValueError("slice_offsets needs one entry more than slice_tenants")
         p, _, dev, keep = _as_pairs(pairs)
         check(self._lib.gs_engine_ingest(self._h, st.ctypes.data, so.ctypes.data, st.size, p, int(dev),
-                                         _stream_ptr(stream)), "gs_engine_ingest")
+                                         _device_stream(stream, dev)), "gs_engine_ingest")
         del keep
 
     def ingest_batches(self, batches, stream=None) -> None:
@@ -160,6 +160,11 @@ class SketchEngine:
         p, _, dev, keep = _as_pairs(pairs)
         if not dev and st.size:
             raise ValueError("phase() takes device-resident records (a CUDA tensor)")
+        if dev:
+            # gs_engine_phase takes no stream: the records' producer (and a .contiguous() copy) must be
+            # complete before the engine's own stream reads them
+            import torch
+            torch.cuda.current_stream().synchronize()
         qt = np.ascontiguousarray(list(query_tenants), dtype=np.uint32)
         ncc = np.zeros(max(qt.size, 1), np.uint32)
         rounds = np.zeros(max(qt.size, 1), np.uint32)

@@ -79,6 +79,17 @@ def _stream_ptr(stream) -> C.c_void_p:
     return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
 
 
+def _device_stream(stream, on_device: bool) -> C.c_void_p:
+    """The stream a call with device operands runs on.  With no explicit stream, torch's current
+    stream: the library's work is then ordered after the torch kernels that produced the operands, and
+    torch's caching allocator, which reuses a freed block only after the work queued on that stream,
+    cannot hand a temporary (a .contiguous() copy) to another tensor while the library still reads it."""
+    if stream is None and on_device:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return _stream_ptr(stream)
+
+
 class GraphSketch:
     """A sketch set of `num_levels` levels of V vertex sketches resident on one GPU."""
 
@@ -130,7 +141,7 @@ class GraphSketch:
     # ---- ingest ----
     def ingest_pairs(self, pairs, stream=None) -> None:
         p, n, dev, keep = _as_pairs(pairs)
-        check(self._lib.gs_ingest_pairs(self._h, p, n, int(dev), _stream_ptr(stream)), "gs_ingest_pairs")
+        check(self._lib.gs_ingest_pairs(self._h, p, n, int(dev), _device_stream(stream, dev)), "gs_ingest_pairs")
         del keep
 
     def ingest_edges(self, src, dst, stream=None) -> None:
@@ -140,7 +151,7 @@ class GraphSketch:
         b, nb, db, kb = _as_u32(dst)
         if na != nb or da != db:
             raise ValueError("src and dst need the same length and the same side (host or device)")
-        check(self._lib.gs_ingest_edges(self._h, a, b, na, int(da), _stream_ptr(stream)), "gs_ingest_edges")
+        check(self._lib.gs_ingest_edges(self._h, a, b, na, int(da), _device_stream(stream, da)), "gs_ingest_edges")
         del ka, kb
 
     def ingest_vertex_batches(self, srcs, starts, sizes, dsts, level: int = 0) -> None:
@@ -271,6 +282,6 @@ def rmat_stream(log2_v: int, n: int, seed: int, first: int = 0, a: float = 0.57,
     p, cnt, dev, keep = _as_pairs(out)
     if cnt < n:
         raise ValueError("output too small")
-    check(lib().gs_gen_rmat_stream(log2_v, a, b, c, delete_frac, seed, first, n, p, int(dev), _stream_ptr(stream)),
-          "gs_gen_rmat_stream")
+    check(lib().gs_gen_rmat_stream(log2_v, a, b, c, delete_frac, seed, first, n, p, int(dev),
+                                   _device_stream(stream, dev)), "gs_gen_rmat_stream")
     return out

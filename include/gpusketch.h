@@ -252,11 +252,15 @@ gs_status gs_profile_read(gs_graph* g, gs_profile* out);
  * device sketches of a connected-components graph, laid out [V][num_buckets] gs_bucket as
  * gs_geometry_for(num_vertices, sketches_factor) sizes them; the result equals gs_ingest_pairs on a
  * gs_graph with the same seed and factor.  Calls no allocator: all scratch is one static device array
- * of about 2.3 MB that every GPU loading the library holds until exit, set up on a device by the
- * first call made there (make that first call before any stream capture).  The array is shared by
- * all calls and keeps the last call's contents, so calls that overlap on the GPU race.  Rejects
- * num_vertices outside [2, GS_NOALLOC_MAX_VERTICES] and n > GS_NOALLOC_MAX_EDGES with GS_ERR_BAD_ARG.
- * Runs on `cuda_stream` (may be NULL) on the current device and returns once the update is applied. */
+ * of about 2.3 MB that every GPU loading the library holds until exit; each call looks up the array's
+ * device address on the current device.  The array is shared by all calls and keeps the last call's
+ * contents, so calls that overlap on the GPU race.  Rejects num_vertices outside
+ * [2, GS_NOALLOC_MAX_VERTICES] and n > GS_NOALLOC_MAX_EDGES with GS_ERR_BAD_ARG before touching the
+ * sketches.  Runs on `cuda_stream` (may be NULL) on the current device and is synchronous: it waits
+ * for that stream to apply the update and check the device error word, so it must not be called while
+ * the stream is being captured into a CUDA graph.  When a record names a vertex >= num_vertices the
+ * call returns GS_ERR_BAD_ARG after applying every other record of the call (only the out-of-range
+ * records are skipped), so a caller that retries must not resend the records that were applied. */
 #define GS_NOALLOC_MAX_VERTICES 65536u
 #define GS_NOALLOC_MAX_EDGES 65536u
 gs_status gs_ingest_pairs_noalloc(uint32_t num_vertices, uint64_t seed, double sketches_factor,

@@ -160,6 +160,32 @@ def test_ingest_edges_src_dst_arrays(restatement, on_device):
         assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs)
 
 
+def test_device_views_produced_just_before_the_call(restatement):
+    """Non-contiguous column views of records that a torch kernel has only just produced, on a side
+    stream: the library orders its work after torch's current stream, and the contiguous temporaries
+    stay valid until it has read them (a freed block is reused right after each call)."""
+    import torch
+    V, seed = 3000, 0x5EED3300
+    side = torch.cuda.Stream()
+    host = []
+    with gs.GraphSketch(V, seed, max_batch_edges=1 << 13) as g:
+        with torch.cuda.stream(side):
+            gen = torch.Generator(device="cuda").manual_seed(77)
+            for k in range(3):
+                recs = torch.randint(0, V, (40_000, 3), device="cuda", dtype=torch.int32, generator=gen)
+                if k % 2:
+                    g.ingest_pairs(recs[:, 1:])               # a strided two-column view
+                else:
+                    g.ingest_edges(recs[:, 0], recs[:, 2])    # strided columns
+                host.append(recs.cpu().numpy())
+                del recs
+                torch.full((1 << 22,), 7, dtype=torch.int32, device="cuda")  # takes freed blocks
+            side.synchronize()
+        got = sketch_bytes(g)
+    pairs = np.concatenate([h[:, [1, 2]] if k % 2 else h[:, [0, 2]] for k, h in enumerate(host)]).astype(np.uint32)
+    assert got == oracle_bytes(restatement, V, seed, pairs)
+
+
 def test_more_than_32_columns(restatement):
     """sketches_factor 3 at V=4096 gives 49 columns: two columns per lane."""
     V, seed, f = 4096, 5, 3.0

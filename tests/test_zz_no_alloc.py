@@ -28,21 +28,28 @@ def test_noalloc_rejects_sizes_beyond_its_maximum():
 
 
 @pytest.mark.gpu
-def test_noalloc_matches_graph_ingest_on_two_calls():
+@pytest.mark.parametrize("V,factor", [(50000, 1.0), (65536, 1.0), (65536, 1.5)])
+def test_noalloc_matches_graph_ingest_on_two_calls(V, factor):
+    """At the vertex limit with full 65536-record batches (every bucketing region at its largest), and
+    with sketches_factor 1.5 (33 columns: two columns per lane), two calls in a row equal the existing
+    entry point byte for byte."""
     import torch
     assert torch.cuda.is_available()
-    V, seed = 50000, 0xABCDEF
-    nb = gs.geometry_for(V).num_buckets
-    rng = np.random.default_rng(21)
+    seed = 0xABCDEF
+    geo = gs.geometry_for(V, factor)
+    assert (geo.num_columns > 32) == (factor > 1.0)
+    nb = geo.num_buckets
+    rng = np.random.default_rng(21 + V)
     hub = np.stack([np.full(9000, 7, np.uint32), rng.integers(0, V, 9000).astype(np.uint32)], 1)
-    batches = [np.concatenate([rng.integers(0, V, size=(50000, 2), dtype=np.uint32), hub]),
+    batches = [np.concatenate([rng.integers(0, V, size=(65536 - 9000, 2), dtype=np.uint32), hub]),
                rng.integers(0, V, size=(65536, 2), dtype=np.uint32)]
+    batches[1][:4] = [[V - 1, 0], [V - 1, V - 2], [0, V - 1], [V - 2, V - 1]]   # the highest vertex ids
     sk = torch.zeros(V * nb * 2, dtype=torch.int64, device="cuda")   # the caller's own sketch buffer
-    with gs.GraphSketch(V, seed) as g:
+    with gs.GraphSketch(V, seed, sketches_factor=factor) as g:
         for b in batches:
             g.ingest_pairs(b)                                        # the existing entry point
             d = torch.from_numpy(b.astype(np.int32)).cuda()
             torch.cuda.synchronize()
-            rc = _call(V, seed, d.data_ptr(), len(b), sk.data_ptr())
+            rc = _call(V, seed, d.data_ptr(), len(b), sk.data_ptr(), factor)
             assert rc == _native.GS_OK, _native.lib().gs_last_error()
             assert sk.cpu().numpy().tobytes() == g.download().tobytes()   # bit-exact, as every test here
