@@ -72,6 +72,7 @@ SIGNATURES = {
     "gs_ingest_edges": (C.c_int, [_P, _P, _P, C.c_uint64, C.c_int, _P]),
     "gs_ingest_vertex_batches": (C.c_int, [_P, C.c_uint32, _P, _P, _P, C.c_uint32, _P, C.c_uint64, C.c_int, _P]),
     "gs_synchronize": (C.c_int, [_P]),
+    "gs_set_device_wait_limit": (C.c_int, [_P, C.c_uint64]),
     "gs_connected_components": (C.c_int, [_P, C.c_uint32, _P, _U32P, _U32P]),
     "gs_point_query": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(C.c_int)]),
     "gs_spanning_forest": (C.c_int, [_P, C.c_uint32, _P, _U64P]),

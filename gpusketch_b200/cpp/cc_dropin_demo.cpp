@@ -26,7 +26,9 @@ int main(int argc, char** argv) {
     const edge_id_t n = stream.edges();
     auto t0 = std::chrono::steady_clock::now();
     for (int q = 1; q <= queries; q++) {
-      const edge_id_t upto = q == queries ? END_OF_STREAM : n * q / queries;
+      // query points as test/cc_alg_test.cpp:318-340 places them: every n / queries records, the
+      // last one at the end of the stream
+      const edge_id_t upto = q == queries ? END_OF_STREAM : (n / queries) * q;
       driver.process_stream_until(upto);
       driver.prep_query(CONNECTIVITY);
       alg.flush_buffers();

@@ -46,7 +46,6 @@ constexpr uint32_t kAccRun = 16;                 // vertices a warp stages in sh
 constexpr uint32_t kAccGrab = 64;                // vertices a warp takes from the shared work counter
 constexpr uint32_t kThreads = 256;
 constexpr uint32_t kWarps = kThreads / 32;
-constexpr uint64_t kBarrierWaitNs = 1000000000ull;  // a barrier wait gives up after about a second
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
@@ -155,7 +154,9 @@ __device__ __forceinline__ void sample_octet(const GsBucket* col, const GsBucket
 // Grid-wide barrier of a co-resident launch.  Returns false when any block gave up waiting.  The
 // waiting thread backs off exponentially (32 ns .. 1 us) so that hundreds of pollers do not saturate
 // the L2 slice that holds the generation word.
-__device__ bool grid_sync(uint32_t* count, uint32_t* gen, uint32_t* err) {
+// wait_ns: how long (summed sleep time) a block waits for the others before it reports
+// GS_DEV_ERR_TIMEOUT and gives up
+__device__ bool grid_sync(uint32_t* count, uint32_t* gen, uint32_t* err, uint64_t wait_ns) {
   __shared__ uint32_t s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -174,7 +175,7 @@ __device__ bool grid_sync(uint32_t* count, uint32_t* gen, uint32_t* err) {
         waited += sleep_ns;
         if (sleep_ns < 1024) sleep_ns <<= 1;
         if ((++it & 63u) == 0 && (ld_volatile(err) & GS_DEV_ERR_TIMEOUT)) { ok = 0; break; }
-        if (waited > kBarrierWaitNs) {
+        if (waited > wait_ns) {
           atomicOr(err, (uint32_t)GS_DEV_ERR_TIMEOUT);
           ok = 0;
           break;
@@ -206,6 +207,7 @@ struct BorArgs {
   uint32_t* status;            // [0] error bits [3] roots [4] forest edges [5] active tenants [6,7] barrier
                                // [12] accumulate work counter
   uint32_t* tstate;            // [T][4]: done, modified this round, rounds, out of samples
+  uint64_t wait_ns;            // grid-barrier wait limit
 };
 
 __device__ __forceinline__ const GsBorTenant& tenant_of(const BorArgs& A, uint32_t t) {
@@ -248,7 +250,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
 
   for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.parent[v] = v;
   if (gtid == 0) *nroots_p = 0;
-  if (!grid_sync(bcount, bgen, err)) return;
+  if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
 
   for (uint32_t round = 0; round < A.max_rounds; round++) {
     snapshot_done(A, s_done);
@@ -274,7 +276,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
           if (fresh) A.roots[at + __popc(fm & ((1u << lane) - 1u))] = r;
         }
       }
-      if (!grid_sync(bcount, bgen, err)) return;
+      if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
 
       // ---- accumulate column r + the deterministic bucket per component ----
       // Warps take runs of kAccGrab vertices from a shared counter (finished tenants' vertices cost
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         }
         if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
       }
-      if (!grid_sync(bcount, bgen, err)) return;
+      if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
     }
 
     // ---- sample every root into samp[root]: roots spread over the warps by list position ----
@@ -437,7 +439,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         for (uint32_t j = lane; j <= T.bkt; j += 32) acc[j] = GsBucket{0, 0};
       }
     }
-    if (!grid_sync(bcount, bgen, err)) return;
+    if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
 
     // ---- union the sampled edges: one thread per root, so many DSU walks are in flight ----
     for (uint32_t k = gtid; k < nroots; k += gthreads) {
@@ -458,7 +460,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         }
       }
     }
-    if (!grid_sync(bcount, bgen, err)) return;
+    if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
 
     // ---- compress, clear the sizes and the root list for the next round, and per tenant stop
     //      at the first unmodified round (the modified flags were final at the last barrier) ----
@@ -489,7 +491,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         atomicSub(&A.status[5], 1u);
       }
     }
-    if (!grid_sync(bcount, bgen, err)) return;
+    if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
     if (ld_volatile(&A.status[5]) == 0) return;
   }
 }
@@ -516,6 +518,7 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
   A.forest_cap = L.forest_cap;
   A.status = L.status;
   A.tstate = L.tstate;
+  A.wait_ns = L.wait_ns;
   int dev = 0;
   GS_CUDA_TRY(cudaGetDevice(&dev));
   const size_t smem = (size_t)((L.T + 3u) & ~3u) * sizeof(uint32_t) + (size_t)kWarps * kAccRun * L.W * sizeof(GsBucket);
@@ -578,6 +581,7 @@ gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStrea
   L.forest_cap = V;
   L.status = g->d_status;
   L.tstate = g->d_status + 8;
+  L.wait_ns = g->wait_ns;
 
   // the kernel expects all-zero accumulator rows and leaves them so when it runs to the end
   if (g->acc_dirty) GS_CUDA_TRY(cudaMemsetAsync(g->d_acc, 0, (size_t)V * (bkt + 1) * sizeof(GsBucket), s));

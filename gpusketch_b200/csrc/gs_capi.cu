@@ -614,6 +614,14 @@ extern "C" gs_status gs_has_cached_query(gs_graph* g, int* cached) {
   return GS_OK;
 }
 
+// ---- bounded device-side waits ----
+
+extern "C" gs_status gs_set_device_wait_limit(gs_graph* g, uint64_t nanoseconds) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  g->wait_ns = nanoseconds ? nanoseconds : kGsDefaultWaitNs;
+  return GS_OK;
+}
+
 // ---- tuning ----
 
 extern "C" gs_status gs_get_tuning(const gs_graph* g, gs_tuning* out) {

@@ -6,6 +6,9 @@
 
 #include "gs_common.cuh"
 
+// Default limit of a bounded device-side wait (the Boruvka grid barriers): about a second.
+constexpr uint64_t kGsDefaultWaitNs = 1000000000ull;
+
 // Column-constant row of one engine tenant: num_columns column constants, then the checksum constant.
 constexpr uint32_t kColStride = 65;
 
@@ -102,6 +105,7 @@ struct gs_graph {
   std::vector<uint32_t> sample_cursor;  // per level: round-0 column of the next k-forest
   bool labels_valid = false;     // d_parent holds the partition of the last query
   uint32_t labels_level = 0;
+  uint64_t wait_ns = kGsDefaultWaitNs;  // limit of the Boruvka kernel's grid-barrier waits
 
   // ---- eager DSU (gs_eager.cu): connectivity kept current by the ingest path ----
   bool eager_on = false;
@@ -217,6 +221,7 @@ struct GsBorLaunch {
   uint32_t forest_cap = 0;
   uint32_t* status = nullptr;            // 8 words: [0] errors [4] forest edges [5] running tenants [6,7] barrier
   uint32_t* tstate = nullptr;            // [T][4]: done, modified, rounds, out of samples
+  uint64_t wait_ns = kGsDefaultWaitNs;   // grid-barrier wait limit
 };
 
 // All Boruvka rounds of every tenant in one cooperative launch (queued on s, no host sync).

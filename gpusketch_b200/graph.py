@@ -211,6 +211,10 @@ class GraphSketch:
         check(self._lib.gs_edge_store_edges(self._h, t, out.ctypes.data, n.value, C.byref(n)), "gs_edge_store_edges")
         return out[: n.value].copy()
 
+    def set_device_wait_limit(self, nanoseconds: int = 0) -> None:
+        """Limit of the Boruvka kernel's grid-barrier waits (0 = the default, about a second)."""
+        check(self._lib.gs_set_device_wait_limit(self._h, nanoseconds), "gs_set_device_wait_limit")
+
     # ---- eager DSU ----
     def set_eager_dsu(self, on: bool = True) -> None:
         """Keep a device DSU current during ingest so that queries skip Boruvka while it is valid."""

@@ -211,6 +211,15 @@ gs_status gs_set_eager_dsu(gs_graph* g, int enable);
  * gs_connected_components will be answered from the eager DSU.  Synchronizes the handle. */
 gs_status gs_has_cached_query(gs_graph* g, int* cached);
 
+/* ---- bounded device-side waits ----
+ * Every wait of a device kernel on other blocks (the grid barriers of the persistent Boruvka kernel)
+ * gives up after a limit, sets a device error bit and lets the kernel return, so a wait that cannot
+ * end leaves the context usable: the query then fails with GS_ERR_TIMEOUT and the next query starts
+ * from scratch.  Sets that limit for this handle's queries (summed sleep time of one wait; default
+ * about one second; 0 restores the default).  Library extension without a reference counterpart;
+ * the tests set a limit far below one barrier's normal wait to make a wait run out. */
+gs_status gs_set_device_wait_limit(gs_graph* g, uint64_t nanoseconds);
+
 /* ---- tuning (set by the autotuner, gpusketch_b200/autotune.py) ---- */
 typedef struct gs_tuning {
   uint32_t chunk;            /* records per sketch-update work item (>= 32) */

@@ -147,6 +147,9 @@ def _bind_ref() -> C.CDLL:
     L.gsref_cc_connected_components.argtypes = [C.c_void_p, _u32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.gsref_cc_spanning_forest.argtypes = [C.c_void_p, _u32, C.POINTER(C.c_uint64)]
     L.gsref_cc_write_binary.argtypes = [C.c_void_p, C.c_char_p]
+    L.gsref_cc_sketch_bytes.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, _u8]
+    L.gsref_mc_ingest_tagged.argtypes = [C.c_void_p, _u32, C.c_uint64, C.c_uint32, C.c_uint32]
+    L.gsref_mc_level_bytes.argtypes = [C.c_void_p, C.c_uint32, _u8]
     L.gsref_cc_from_file.restype = C.c_void_p
     L.gsref_cc_from_file.argtypes = [C.c_char_p]
     L.gsref_mc_new.restype = C.c_void_p
@@ -246,6 +249,14 @@ class RefCC:
     def sketch_bytes(self) -> bytes:
         return self.write_binary_bytes()[20:]
 
+    def sketch_array(self, num_buckets: int, first: int = 0, count: int | None = None) -> np.ndarray:
+        """The reference Sketch objects' bucket arrays of vertices [first, first+count) as
+        (count, num_buckets * 2) uint64, read from memory (no file)."""
+        count = self.V - first if count is None else count
+        out = np.empty((count, num_buckets * 2), np.uint64)
+        self.L.gsref_cc_sketch_bytes(self.h, first, count, out.view(np.uint8).reshape(-1))
+        return out
+
 
 class RefMC:
     """The reference's own MCSketchAlg with `num_graphs` host sketch subgraphs."""
@@ -253,7 +264,19 @@ class RefMC:
     def __init__(self, V: int, seed: int, num_graphs: int, factor: float = 1.0):
         self.L = _bind_ref()
         self.V = V
+        self.num_graphs = num_graphs
         self.h = self.L.gsref_mc_new(V, seed & (2**64 - 1), num_graphs, factor)
+
+    def ingest_tagged(self, pairs: np.ndarray, num_subgraphs: int) -> None:
+        """Every record into sketch graphs 0..min(tag, num_graphs-1), tag = the reference's
+        get_index_depth(edge id, seed, num_subgraphs-1), through MCSketchAlg::update_subgraph."""
+        p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1)
+        self.L.gsref_mc_ingest_tagged(self.h, p, p.size // 2, num_subgraphs, self.num_graphs)
+
+    def level_bytes(self, graph_id: int, num_buckets: int) -> bytes:
+        out = np.empty(self.V * num_buckets * 16, np.uint8)
+        self.L.gsref_mc_level_bytes(self.h, graph_id, out)
+        return out.tobytes()
 
     def close(self):
         if self.h:

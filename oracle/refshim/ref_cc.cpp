@@ -11,8 +11,13 @@
 #include <vector>
 
 #include "cc_sketch_alg.h"
+#include "private_access.h"
 
 static thread_local std::string g_err;
+
+// CCSketchAlg::sketches (include/cc_sketch_alg.h:76)
+struct GsCCSketches { typedef Sketch** CCSketchAlg::*type; friend type gs_ref_member(GsCCSketches); };
+template struct GsRefPrivate<GsCCSketches, &CCSketchAlg::sketches>;
 
 extern "C" {
 
@@ -95,6 +100,20 @@ int gsref_cc_spanning_forest(void* h, uint32_t* edges, uint64_t* n) {
     *n = es.size();
   } catch (OutOfSamplesException& e) { g_err = e.what(); return 2; }
   catch (std::exception& e) { g_err = e.what(); return 1; }
+  return 0;
+}
+
+// The bucket arrays of vertices [first, first+count) back to back (Sketch::serialize layout,
+// src/sketch.cpp:204-206), straight from the reference's own Sketch objects.
+int gsref_cc_sketch_bytes(void* h, uint32_t first, uint32_t count, uint8_t* out) {
+  auto* a = static_cast<CCSketchAlg*>(h);
+  Sketch** sk = a->*gs_ref_member(GsCCSketches());
+  size_t pos = 0;
+  for (uint32_t v = first; v < first + count; v++) {
+    const size_t nb = sk[v]->bucket_array_bytes();
+    std::memcpy(out + pos, sk[v]->get_readonly_bucket_ptr(), nb);
+    pos += nb;
+  }
   return 0;
 }
 

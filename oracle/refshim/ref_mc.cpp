@@ -1,12 +1,18 @@
 // extern "C" wrappers over the reference's own MCSketchAlg (compiled from the reference's
 // sources by oracle/Makefile).  TEST INFRASTRUCTURE ONLY.  Sketches are plain host Sketches
 // (SketchParams::cudaUVM_enabled = false, src/mc_sketch_alg.cpp:114-119).
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <string>
 #include <vector>
 
 #include "mc_sketch_alg.h"
+#include "private_access.h"
+
+// MCSketchAlg::sketches (include/mc_sketch_alg.h:86): graph g's vertex v at [g*V + v]
+struct GsMCSketches { typedef Sketch** MCSketchAlg::*type; friend type gs_ref_member(GsMCSketches); };
+template struct GsRefPrivate<GsMCSketches, &MCSketchAlg::sketches>;
 
 extern "C" {
 
@@ -24,6 +30,37 @@ void gsref_mc_free(void* h) { delete static_cast<MCSketchAlg*>(h); }
 
 void gsref_mc_update(void* h, uint32_t graph_id, uint32_t src, uint32_t dst) {
   static_cast<MCSketchAlg*>(h)->update_subgraph((int)graph_id, {{src, dst}, INSERT});
+}
+
+// The reference GPU driver's subgraph fan-out, on the host: record (src, dst) gets the tag
+// get_index_depth(concat_pairing_fn(src, dst), seed, num_subgraphs - 1) and is inserted into sketch
+// graphs 0 .. min(tag, num_graphs - 1) (MCGPUSketchAlg::apply_update_batch and
+// complete_update_batch, src/mc_gpu_sketch_alg.cpp:139-178,83-137; every subgraph stays sketched).
+void gsref_mc_ingest_tagged(void* h, const uint32_t* pairs, uint64_t n, uint32_t num_subgraphs,
+                            uint32_t num_graphs) {
+  auto* a = static_cast<MCSketchAlg*>(h);
+  const size_t seed = a->get_seed();
+  for (uint64_t i = 0; i < n; i++) {
+    const node_id_t u = pairs[2 * i], v = pairs[2 * i + 1];
+    const vec_t e = static_cast<vec_t>(concat_pairing_fn(u, v));
+    const size_t tag = Bucket_Boruvka::get_index_depth(e, seed, num_subgraphs - 1);
+    const size_t top = std::min<size_t>(tag, num_graphs - 1);
+    for (size_t g = 0; g <= top; g++) a->update_subgraph((int)g, {{u, v}, INSERT});
+  }
+}
+
+// Sketch bytes of graph g, vertices 0..V-1 back to back (Sketch::serialize layout).
+int gsref_mc_level_bytes(void* h, uint32_t graph_id, uint8_t* out) {
+  auto* a = static_cast<MCSketchAlg*>(h);
+  Sketch** sk = a->*gs_ref_member(GsMCSketches());
+  const node_id_t V = a->get_num_vertices();
+  size_t pos = 0;
+  for (node_id_t v = 0; v < V; v++) {
+    const Sketch* s = sk[(size_t)graph_id * V + v];
+    std::memcpy(out + pos, s->get_readonly_bucket_ptr(), s->bucket_array_bytes());
+    pos += s->bucket_array_bytes();
+  }
+  return 0;
 }
 
 // k disjoint spanning forests of subgraph graph_id; forest f goes to edges + f*2*(V-1).

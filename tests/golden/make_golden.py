@@ -1,7 +1,9 @@
-"""Generates the golden fixtures in tests/golden/ (run in the build container, where the reference
-tree and python-xxhash are available):
+"""Generates the golden fixtures in tests/golden/ (run where the reference tree and python-xxhash are
+available):
 
-    python tests/golden/make_golden.py
+    GS_REFERENCE_TREE=<reference checkout> python tests/golden/make_golden.py
+
+GS_REFERENCE_TREE defaults to a directory named `reference` beside this repository's root.
 
 * xxh3_vectors.json   XXH3_64bits_withSeed of 8-byte keys from python-xxhash (libxxhash), the hash
                       the reference binds in include/types.h:8-9.
@@ -15,8 +17,13 @@ tree and python-xxhash are available):
                       rebuilt from that rule and checked against the reference file here; the record
                       order and the delete/reinsert churn (6867 inserts, 1661 deletes, as in
                       multiples_graph_1024_stream.data) are our own seeded choice.
+* multiples_graph_1024_stream.data
+                      the reference's own binary stream fixture (test/res/multiples_graph_1024_stream.data,
+                      replayed by test/cc_alg_test.cpp:300-350), copied byte for byte: {u32 V, u64 n}
+                      then n packed {u8 type, u32 src, u32 dst} records.
 * ref_digests.json    sha256 of the reference CCSketchAlg's write_binary sketch bytes, its component
-                      count and Boruvka rounds, for seeded streams (the plain-CC ER stream among them).
+                      count and Boruvka rounds, for seeded streams (the plain-CC ER stream among them)
+                      and for the records of the reference's binary fixture in file order.
 """
 from __future__ import annotations
 
@@ -31,8 +38,18 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+from stream_file import read_stream_file  # noqa: E402
 
-REF_TREE = os.environ.get("GS_REFERENCE_TREE", "/root/reference")
+REF_TREE = os.environ.get("GS_REFERENCE_TREE", os.path.join(os.path.dirname(ROOT), "reference"))
+FIXTURE = "multiples_graph_1024_stream.data"
+
+
+def copy_reference_fixture() -> None:
+    with open(os.path.join(REF_TREE, "test", "res", FIXTURE), "rb") as f:
+        data = f.read()
+    with open(os.path.join(HERE, FIXTURE), "wb") as f:
+        f.write(data)
 
 
 def multiples_edges(V: int = 1024) -> np.ndarray:
@@ -127,6 +144,7 @@ def ref_digests() -> list:
         ("er256_sparse", 256, 7, lambda: gs.er_stream(256, 0.01, 11, 0.5, 0.2)),
         ("er4096", 4096, 0x1234_5678_9ABC_DEF0, lambda: gs.er_stream(4096, 0.002, 13, 0.1, 0.5)),
         ("rmat_v2p12", 4096, 2**63 + 5, lambda: gs.rmat_stream(12, 40000, 0x5EED0002)),
+        ("multiples_file_1024", 1024, 0xC0FFEE, lambda: read_stream_file(os.path.join(HERE, FIXTURE))[2]),
     ]
     out = []
     for name, V, seed, mk in cases:
@@ -147,6 +165,7 @@ def main() -> None:
     edges = multiples_edges()
     if os.path.isdir(REF_TREE):
         check_against_reference_fixture(edges)
+        copy_reference_fixture()
     np.save(os.path.join(HERE, "multiples_1024_stream.npy"), multiples_stream())
     with open(os.path.join(HERE, "xxh3_vectors.json"), "w") as f:
         json.dump(xxh3_vectors(), f, indent=0)

@@ -10,21 +10,10 @@ import subprocess
 import numpy as np
 import pytest
 
+from stream_file import write_stream_file
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DEMO = os.path.join(ROOT, "gpusketch_b200", "_build", "cc_dropin_demo")
-
-
-def write_stream(path, V, pairs):
-    """StreamingUtilities binary stream: {u32 V, u64 n} then {u8 type, u32 src, u32 dst} records;
-    a record is a delete when it toggles an edge that is present."""
-    present = set()
-    with open(path, "wb") as f:
-        f.write(struct.pack("<IQ", V, len(pairs)))
-        for a, b in pairs.tolist():
-            e = (min(a, b), max(a, b))
-            t = 1 if e in present else 0
-            present.symmetric_difference_update({e})
-            f.write(struct.pack("<BII", t, a, b))
 
 
 @pytest.mark.gpu
@@ -34,7 +23,7 @@ def test_cpp_dropin_driver_matches_reference(tmp_path, golden_dir):
     pairs = np.load(os.path.join(golden_dir, "multiples_1024_stream.npy"))
     stream = str(tmp_path / "multiples.data")
     ck = str(tmp_path / "ck.bin")
-    write_stream(stream, 1024, pairs)
+    write_stream_file(stream, 1024, pairs)
     out = subprocess.run([DEMO, stream, str(int(case["seed"])), ck, "3"], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr
     lines = [l for l in out.stdout.splitlines() if l.startswith("num_cc=")]
@@ -48,7 +37,7 @@ def test_stream_file_format_roundtrip(tmp_path):
     """The writer above produces the format the reference's fixture uses (9-byte records)."""
     pairs = np.array([[1, 2], [2, 1], [3, 4]], np.uint32)
     p = str(tmp_path / "s.data")
-    write_stream(p, 8, pairs)
+    write_stream_file(p, 8, pairs)
     d = open(p, "rb").read()
     assert len(d) == 12 + 9 * 3
     assert struct.unpack_from("<IQ", d, 0) == (8, 3)

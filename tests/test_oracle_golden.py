@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from oracle import Restatement, ref_available
+from stream_file import REFERENCE_FIXTURE, read_stream_file
 
 
 def test_xxh3_golden_vectors(restatement, golden_dir):
@@ -63,6 +64,8 @@ def test_sketch_digests_match_reference(restatement, golden_dir):
             pairs = gs.er_stream(256, 0.01, 11, 0.5, 0.2)
         elif case["name"] == "er4096":
             pairs = gs.er_stream(4096, 0.002, 13, 0.1, 0.5)
+        elif case["name"] == "multiples_file_1024":
+            pairs = read_stream_file(REFERENCE_FIXTURE)[2]
         else:
             pairs = gs.rmat_stream(12, 40000, 0x5EED0002)
         assert hashlib.sha256(np.ascontiguousarray(pairs, np.uint32).tobytes()).hexdigest() == case["pairs_sha256"]
@@ -121,3 +124,71 @@ def test_restatement_k_forests_are_disjoint_spanning_forests(restatement):
         ref.update(0, a, b)
     rc, rforests = ref.k_forests(0, k)
     assert rc == 0 and [len(f) for f in rforests] == [len(f) for f in forests]
+
+
+def test_reference_stream_fixture(restatement, golden_dir):
+    """The reference's own binary fixture (test/res/multiples_graph_1024_stream.data, copied verbatim):
+    8528 records of which 1661 deletes, each delete toggling a present edge, ending at the multiples
+    graph of test/res/multiples_graph_1024.txt (78 components, test/cc_alg_test.cpp:300-350).  The
+    restatement's sketch bytes equal the reference digest, and at each of the reference test's ten query
+    points its Boruvka partition equals the exact partition of the prefix."""
+    import hashlib
+    V, types, pairs = read_stream_file(REFERENCE_FIXTURE)
+    assert (V, len(pairs), int((types == 1).sum())) == (1024, 8528, 1661)
+    present = set()
+    for t, (a, b) in zip(types.tolist(), pairs.tolist()):
+        e = (min(a, b), max(a, b))
+        assert (t == 1) == (e in present)
+        present.symmetric_difference_update({e})
+    rule = {(i, j) for i in range(2, 1024) for j in range(2 * i, 1024, i)}
+    assert present == rule
+    case = [c for c in json.load(open(os.path.join(golden_dir, "ref_digests.json")))
+            if c["name"] == "multiples_file_1024"][0]
+    sk = restatement.new_sketches(V)
+    restatement.ingest(sk, V, 0xC0FFEE, pairs)
+    assert hashlib.sha256(sk.tobytes()).hexdigest() == case["sketch_sha256"]
+    per = len(pairs) // 10
+    for q in range(1, 11):
+        upto = per * q if q < 10 else len(pairs)
+        sk = restatement.new_sketches(V)
+        restatement.ingest(sk, V, 0xC0FFEE, pairs[:upto])
+        st, labels, _, _ = restatement.boruvka(sk, V, 0xC0FFEE)
+        n, exact = restatement.exact_cc(V, pairs[:upto])
+        assert st == 0 and np.array_equal(labels, exact), q
+    assert n == 78
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+def test_reference_fixture_through_reference_batches(restatement, golden_dir):
+    """The reference's CCSketchAlg fed the fixture's records the way its driver does (both directions,
+    per source vertex, through apply_update_batch) gives the digest's bytes."""
+    import hashlib
+    from oracle import RefCC
+    V, _, pairs = read_stream_file(REFERENCE_FIXTURE)
+    case = [c for c in json.load(open(os.path.join(golden_dir, "ref_digests.json")))
+            if c["name"] == "multiples_file_1024"][0]
+    ref = RefCC(V, 0xC0FFEE, 1.0, workers=4)
+    ref.ingest(pairs, threads=4)
+    assert hashlib.sha256(ref.sketch_bytes()).hexdigest() == case["sketch_sha256"]
+    labels, ncc, rounds = ref.connected_components()
+    assert (ncc, rounds) == (case["num_cc"], case["rounds"]) == (78, 6)
+    ref.close()
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+def test_min_cut_level_fanout_equals_reference(restatement):
+    """The restatement's subgraph tagging (levels 0..min(tag, levels-1), tag = get_index_depth(e, seed,
+    L-1)) equals the reference MCSketchAlg fed through the reference GPU driver's fan-out
+    (src/mc_gpu_sketch_alg.cpp:139-178) level by level."""
+    from oracle import RefMC
+    for V, seed, levels, L, n in [(600, 17, 5, 19, 20000), (1000, 2**63 + 11, 3, 21, 30000)]:
+        rng = np.random.default_rng(V)
+        pairs = rng.integers(0, V, size=(n, 2), dtype=np.uint32)
+        ref = RefMC(V, seed, levels)
+        ref.ingest_tagged(pairs, L)
+        nb = restatement.geometry(V)["num_buckets"]
+        sk = restatement.new_sketches(V, levels=levels)
+        restatement.ingest_levels(sk, V, levels, L, seed, pairs)
+        for g in range(levels):
+            assert ref.level_bytes(g, nb) == sk[g * V * nb * 2:(g + 1) * V * nb * 2].tobytes(), (V, g)
+        ref.close()
