@@ -9,7 +9,8 @@ One step = clear the V sketches, then 8 x (ingest 2^27 records + connected_compo
 (8 GiB per GPU) are resident in HBM before timing and larger than L2.  `value` is the edge-update rate
 of the K timed steps (CUDA events on the stream the library launches on; max over ranks); `e2e` is the
 same workload through the C ABI from pinned host buffers (H2D inside the timed region) with the
-component labels copied back after every query.  N > 1 ranks run independent replicas (seed + rank).
+component labels copied back after every query; each phase's query is queued (gs_connected_components_async)
+and the next phase's records are queued behind it (gs_ingest_pairs_async) before its answer is collected.  N > 1 ranks run independent replicas (seed + rank).
 `--impl reference` times the reference's own CPU CCSketchAlg (compiled from its sources into
 oracle/_ref) on a bounded sample of the same stream with every host thread.
 """
@@ -489,10 +490,15 @@ def run_gs(args):
         labels_host = torch.empty(V, dtype=torch.int32, pin_memory=True)
 
         def step_e2e():
+            # each phase's query is queued behind its records, then the next phase's records (copies
+            # included) are queued behind the query, so the copy engine never waits for a query
             g.clear()
+            g.ingest_pairs_async(h_in[0:phase])                    # host pinned -> H2D inside the library
             for p in range(P):
-                g.ingest_pairs(h_in[p * phase:(p + 1) * phase])   # host pinned -> H2D inside the library
-                labels, _, _ = g.connected_components()           # labels copied back to the host
+                g.connected_components_async()
+                if p + 1 < P:
+                    g.ingest_pairs_async(h_in[(p + 1) * phase:(p + 2) * phase])
+                labels, _, _ = g.query_wait()                      # labels copied back to the host
         step_e2e()
         torch.cuda.synchronize()
         barrier()

@@ -8,7 +8,10 @@
 // Bulk edge records (the device-bucketed path) go through ingest_records.
 #pragma once
 
+#include <chrono>
+#include <iostream>
 #include <mutex>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -28,6 +31,22 @@ class CCGPUSketchAlg {
     cfg.device = device;
     gs_throw_if(gs_graph_create(&cfg, &g), "gs_graph_create");
     flush_at = 540 * get_desired_updates_per_batch();
+  }
+
+  // The reference's constructor (include/cc_gpu_sketch_alg.h:36, called by tools/cuda_process_stream.cu:126):
+  // the sketch seed comes from the SketchParams; the geometry is derived from num_nodes and
+  // config.sketches_factor, which gives the sizes the tools compute into the SketchParams.  num_updates
+  // only sized the reference's host buffers; num_threads worker threads may call apply_update_batch.
+  CCGPUSketchAlg(node_id_t num_nodes, size_t num_updates, int num_threads, SketchParams sketch_params,
+                 CCAlgConfiguration config = CCAlgConfiguration())
+      : CCGPUSketchAlg(num_nodes, sketch_params.seed, config) {
+    (void)num_updates;
+    num_host_threads = num_threads > 0 ? num_threads : 1;
+    gs_geometry geo{};
+    gs_graph_geometry(g, &geo);
+    if ((sketch_params.num_buckets && sketch_params.num_buckets != geo.num_buckets) ||
+        (sketch_params.num_columns && sketch_params.num_columns != geo.num_columns))
+      throw std::invalid_argument("SketchParams geometry differs from the one num_nodes and sketches_factor give");
   }
 
   ~CCGPUSketchAlg() { gs_graph_destroy(g); }
@@ -91,12 +110,28 @@ class CCGPUSketchAlg {
     gs_throw_if(gs_ingest_pairs(g, pairs, n, 0, nullptr), "gs_ingest_pairs");
   }
 
+  // records [first, first+count) of a binary stream file, read by the library (gs_ingest_stream_file)
+  void ingest_stream_file(const std::string& path, edge_id_t first, edge_id_t count) {
+    std::lock_guard<std::mutex> lk(mtx);
+    gs_throw_if(gs_ingest_stream_file(g, path.c_str(), first, count, nullptr), "gs_ingest_stream_file");
+  }
+
+  // CCGPUSketchAlg::display_time (src/cc_gpu_sketch_alg.cpp:34-75): what the device path did so far
+  void display_time() {
+    gs_profile p{};
+    gs_throw_if(gs_profile_read(g, &p), "gs_profile_read");
+    std::cout << "Device ingest: " << p.records_ingested << " edge records, " << p.ingest_launches
+              << " sketch-update launches, " << p.kernel_launches << " kernel launches\n";
+  }
+
   // ---- queries (src/cc_sketch_alg.cpp:542-683) ----
   ConnectedComponents connected_components() {
     flush_buffers();
     std::vector<node_id_t> labels(num_vertices);
     uint32_t ncc = 0, rounds = 0;
+    cc_alg_start = std::chrono::steady_clock::now();
     gs_throw_if(gs_connected_components(g, 0, labels.data(), &ncc, &rounds), "gs_connected_components");
+    cc_alg_end = std::chrono::steady_clock::now();
     last_query_rounds = rounds;
     return ConnectedComponents(std::move(labels));
   }
@@ -144,6 +179,9 @@ class CCGPUSketchAlg {
   gs_graph* handle() { return g; }
 
   size_t last_query_rounds = 0;
+  // time hooks of the last connected_components() (include/cc_sketch_alg.h:252-253)
+  std::chrono::steady_clock::time_point cc_alg_start;
+  std::chrono::steady_clock::time_point cc_alg_end;
 
  private:
   CCGPUSketchAlg(gs_graph* h, node_id_t V, CCAlgConfiguration cfg) : num_vertices(V), seed(0), config(cfg), g(h) {
@@ -174,6 +212,7 @@ class CCGPUSketchAlg {
   std::mutex mtx;
   bool update_locked = false;
   size_t flush_at = 1;
+  int num_host_threads = 1;
   std::vector<uint32_t> srcs;
   std::vector<uint64_t> starts, sizes;
   std::vector<uint32_t> dsts;

@@ -9,6 +9,8 @@
 #pragma once
 
 #include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <iostream>
 #include <map>
@@ -22,6 +24,50 @@
 typedef uint32_t node_id_t;
 typedef uint64_t edge_id_t;
 typedef uint64_t vec_t;
+typedef uint64_t vec_hash_t;
+
+// include/bucket.h:7-12: the 16-byte bucket of a vertex sketch, laid out as gs_bucket.
+struct Bucket {
+  vec_t alpha;
+  vec_hash_t gamma;
+};
+static_assert(sizeof(Bucket) == sizeof(gs_bucket), "Bucket must match gs_bucket");
+
+// The sizing functions of the reference's Sketch (include/sketch.h:63-77,196-215), which tools call to
+// fill a SketchParams: num_samples = max(18, ceil(f log2 V / (1 - log2 1.2))), one column per sample,
+// bkt_per_col = ceil(log2(V(V-1)/2)) + 1, bumped by one when it is a multiple of 16.  The library
+// derives the same geometry from num_vertices and sketches_factor (gs_geometry_for).
+class Sketch {
+ public:
+  static constexpr size_t default_cols_per_sample = 1;
+  static vec_t calc_vector_length(node_id_t num_vertices) {
+    return (vec_t)std::ceil(double(num_vertices) * (num_vertices - 1) / 2);
+  }
+  static size_t calc_cc_samples(node_id_t num_vertices, double f) {
+    gs_geometry g{};
+    if (gs_geometry_for(num_vertices, f, &g) != GS_OK) return 18;
+    return g.num_samples;
+  }
+  static size_t calc_bkt_per_col(size_t n) {
+    const size_t t = (size_t)std::ceil(std::log2((double)n)) + 1;
+    return t % 16 == 0 ? t + 1 : t;
+  }
+};
+
+// include/cuda_kernel.cuh:23-37: the sketch parameters the reference's tools fill and hand to
+// CCGPUSketchAlg / MCGPUSketchAlg.  The library uses `seed` and derives the geometry from the vertex
+// count and the configuration's sketches_factor (the same numbers the tools compute); the UVM and
+// device-bucket pointers are accepted and left untouched: the sketches live in HBM owned by the library.
+struct SketchParams {
+  size_t num_samples = 0;
+  size_t num_buckets = 0;
+  size_t num_columns = 0;
+  size_t bkt_per_col = 0;
+  size_t seed = 0;
+  bool cudaUVM_enabled = false;
+  Bucket* cudaUVM_buckets = nullptr;
+  Bucket* d_buckets = nullptr;
+};
 
 struct Edge {
   node_id_t src = 0;

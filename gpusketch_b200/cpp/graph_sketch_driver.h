@@ -1,112 +1,47 @@
-// graph_sketch_driver.h - GraphSketchDriver drop-in and the binary stream reader.
+// graph_sketch_driver.h - GraphSketchDriver drop-in.
 //
 // The reference driver (include/graph_sketch_driver.h:70-232) pushes every stream update into a
 // guttering system on the host, and worker threads hand per-vertex batches to
-// Alg::apply_update_batch.  Here the grouping by endpoint happens on the device, so reader threads
-// gather raw (src, dst) records and hand them in bulk to Alg::ingest_records; batch_callback keeps
-// the reference's per-vertex entry for callers that already hold vertex batches.
-//
-// BinaryFileStream reads the StreamingUtilities binary stream format used by the reference's
-// tools and tests (test/res/multiples_graph_1024_stream.data): a header {u32 num_vertices,
-// u64 num_updates} followed by packed 9-byte records {u8 type (0 insert, 1 delete), u32 src,
-// u32 dst}.
+// Alg::apply_update_batch.  Here the grouping by endpoint happens on the device:
+//   * a BinaryFileStream whose algorithm can ingest a file range (Alg::ingest_stream_file) is read by
+//     the library itself (gs_ingest_stream_file: file -> page-locked ring -> device decode and
+//     bucketing), with no per-update host work;
+//   * any other stream is read by the reader threads, which gather raw (src, dst) records and hand
+//     them in bulk to Alg::ingest_records.
+// batch_callback keeps the reference's per-vertex entry for callers that already hold vertex batches.
 #pragma once
+
+#include <unistd.h>
 
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <iostream>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
+#include "binary_file_stream.h"
 #include "gpusketch_types.h"
 
-constexpr edge_id_t END_OF_STREAM = (edge_id_t)-1;
-
-class GraphStream {
- public:
-  virtual ~GraphStream() = default;
-  virtual node_id_t vertices() = 0;
-  virtual edge_id_t edges() = 0;
-  // fills up to `n` updates; a BREAKPOINT update marks the break point / end of the stream
-  virtual size_t get_update_buffer(GraphStreamUpdate* buf, size_t n) = 0;
-  virtual bool set_break_point(edge_id_t idx) = 0;
-  virtual bool get_update_is_thread_safe() { return true; }
-};
-
-class BinaryFileStream : public GraphStream {
- public:
-  explicit BinaryFileStream(const std::string& path) {
-    f = std::fopen(path.c_str(), "rb");
-    if (!f) throw std::runtime_error("cannot open stream file " + path);
-    uint8_t hdr[12];
-    if (std::fread(hdr, 1, 12, f) != 12) throw std::runtime_error("truncated stream header in " + path);
-    std::memcpy(&num_vertices, hdr, 4);
-    std::memcpy(&num_updates, hdr + 4, 8);
-    break_idx = num_updates;
-  }
-  ~BinaryFileStream() override {
-    if (f) std::fclose(f);
-  }
-  node_id_t vertices() override { return num_vertices; }
-  edge_id_t edges() override { return num_updates; }
-
-  bool set_break_point(edge_id_t idx) override {
-    std::lock_guard<std::mutex> lk(mtx);
-    if (idx != END_OF_STREAM && idx < next) return false;
-    break_idx = idx == END_OF_STREAM ? num_updates : std::min<edge_id_t>(idx, num_updates);
-    return true;
-  }
-
-  size_t get_update_buffer(GraphStreamUpdate* buf, size_t n) override {
-    std::lock_guard<std::mutex> lk(mtx);
-    if (n == 0) return 0;
-    const edge_id_t left = break_idx - next;
-    if (left == 0) {
-      buf[0].type = BREAKPOINT;
-      buf[0].edge = {0, 0};
-      return 1;
-    }
-    const size_t m = (size_t)std::min<edge_id_t>(left, n);
-    raw.resize(m * 9);
-    if (std::fseek(f, (long)(12 + next * 9), SEEK_SET) != 0 || std::fread(raw.data(), 9, m, f) != m)
-      throw std::runtime_error("stream file read failed");
-    for (size_t i = 0; i < m; i++) {
-      buf[i].type = raw[9 * i];
-      std::memcpy(&buf[i].edge.src, &raw[9 * i + 1], 4);
-      std::memcpy(&buf[i].edge.dst, &raw[9 * i + 5], 4);
-    }
-    next += m;
-    return m;
-  }
-
-  // writes a stream file in the same format (test and tool helper)
-  static void write(const std::string& path, node_id_t V, const std::vector<GraphStreamUpdate>& ups) {
-    FILE* o = std::fopen(path.c_str(), "wb");
-    if (!o) throw std::runtime_error("cannot create " + path);
-    uint64_t n = ups.size();
-    std::fwrite(&V, 4, 1, o);
-    std::fwrite(&n, 8, 1, o);
-    for (const auto& u : ups) {
-      std::fwrite(&u.type, 1, 1, o);
-      std::fwrite(&u.edge.src, 4, 1, o);
-      std::fwrite(&u.edge.dst, 4, 1, o);
-    }
-    std::fclose(o);
-  }
-
- private:
-  FILE* f = nullptr;
-  node_id_t num_vertices = 0;
-  edge_id_t num_updates = 0;
-  edge_id_t next = 0;
-  edge_id_t break_idx = 0;
-  std::mutex mtx;
-  std::vector<uint8_t> raw;
-};
-
 enum GutterSystem { GUTTERTREE, STANDALONE, CACHETREE };
+
+// The guttering system's settings (GutterTree's GutteringConfiguration, used by the reference's tools,
+// tools/cuda_process_stream.cu:121).  Accepted for source compatibility: records are grouped by endpoint
+// on the device, so there are no host gutters to configure.
+class GutteringConfiguration {
+ public:
+  GutteringConfiguration& page_factor(int) { return *this; }
+  GutteringConfiguration& buffer_exp(int) { return *this; }
+  GutteringConfiguration& fanout(int) { return *this; }
+  GutteringConfiguration& num_flushers(int) { return *this; }
+  GutteringConfiguration& gutter_factor(float) { return *this; }
+  GutteringConfiguration& queue_factor(int) { return *this; }
+  GutteringConfiguration& wq_batch_per_elm(int) { return *this; }
+};
 
 // include/driver_configuration.h:12-48.  The gutter choice is accepted for source compatibility;
 // records are grouped by endpoint on the device whatever it says.
@@ -115,6 +50,7 @@ class DriverConfiguration {
   DriverConfiguration& gutter_sys(GutterSystem s) { _gutter_sys = s; return *this; }
   DriverConfiguration& disk_dir(std::string d) { _disk_dir = std::move(d); return *this; }
   DriverConfiguration& worker_threads(size_t n) { _num_worker_threads = n ? n : 1; return *this; }
+  GutteringConfiguration& gutter_conf() { return _gutter_conf; }
   GutterSystem get_gutter_sys() const { return _gutter_sys; }
   std::string get_disk_dir() const { return _disk_dir; }
   size_t get_worker_threads() const { return _num_worker_threads; }
@@ -123,7 +59,15 @@ class DriverConfiguration {
   GutterSystem _gutter_sys = STANDALONE;
   std::string _disk_dir = ".";
   size_t _num_worker_threads = 1;
+  GutteringConfiguration _gutter_conf;
 };
+
+// Alg::ingest_stream_file(path, first, count) exists
+template <class Alg, class = void>
+struct GsIngestsFiles : std::false_type {};
+template <class Alg>
+struct GsIngestsFiles<Alg, std::void_t<decltype(std::declval<Alg&>().ingest_stream_file(
+                               std::declval<const std::string&>(), edge_id_t(), edge_id_t()))>> : std::true_type {};
 
 template <class Alg>
 class GraphSketchDriver {
@@ -140,6 +84,16 @@ class GraphSketchDriver {
   void process_stream_until(edge_id_t break_edge_idx) {
     if (!stream->set_break_point(break_edge_idx))
       throw std::runtime_error("Could not correctly set breakpoint: " + std::to_string(break_edge_idx));
+    if constexpr (GsIngestsFiles<Alg>::value) {
+      if (auto* file = dynamic_cast<BinaryFileStream*>(stream)) {
+        edge_id_t first = 0, n = 0;
+        if (file->claim(&first, &n)) {
+          alg->ingest_stream_file(file->path(), first, n);
+          total_updates += 2 * n;
+        }
+        return;
+      }
+    }
     auto task = [&]() {
       std::vector<GraphStreamUpdate> buf(update_array_size);
       std::vector<uint32_t> pairs;

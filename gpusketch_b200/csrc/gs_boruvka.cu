@@ -553,7 +553,7 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
   return GS_OK;
 }
 
-gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s) {
+gs_status gs_boruvka_enqueue(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s, uint32_t* h_out) {
   const uint32_t V = g->V, nb = g->geom.num_buckets, bkt = g->geom.bkt_per_col;
   g->labels_valid = false;
   g->last_forest_edges = 0;
@@ -586,7 +586,9 @@ gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStrea
   // the kernel expects all-zero accumulator rows and leaves them so when it runs to the end
   if (g->acc_dirty) GS_CUDA_TRY(cudaMemsetAsync(g->d_acc, 0, (size_t)V * (bkt + 1) * sizeof(GsBucket), s));
   g->acc_dirty = true;
-  // status: everything zero except the count of tenants still running
+  // the ingest error bits not yet reported move to word 16 (read back with the query's words);
+  // status: everything else zero except the count of tenants still running
+  GS_CUDA_TRY(cudaMemcpyAsync(g->d_status + 16, g->d_status, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
   g->h_status[15] = 1;
   GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 16 * sizeof(uint32_t), s));
   GS_CUDA_TRY(cudaMemcpyAsync(g->d_status + 5, g->h_status + 15, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
@@ -594,9 +596,11 @@ gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStrea
     GsProfScope ps(g, GS_PROF_QUERY, s, 1);
     GS_TRY(gs_boruvka_launch(L, s));
   }
-  GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, 15 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  GS_CUDA_TRY(cudaStreamSynchronize(s));
-  const uint32_t* st = g->h_status;
+  GS_CUDA_TRY(cudaMemcpyAsync(h_out, g->d_status, 17 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  return GS_OK;
+}
+
+gs_status gs_boruvka_finish(gs_graph* g, uint32_t level, const uint32_t* st) {
   if (st[0] & GS_DEV_ERR_TIMEOUT) {
     gs_set_error("a grid barrier of the Boruvka kernel gave up waiting");
     return GS_ERR_TIMEOUT;
@@ -611,8 +615,14 @@ gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStrea
     return GS_ERR_SKETCH_FAIL;
   }
   g->last_rounds = st[8 + 2];
-  g->last_forest_edges = st[4] < V ? st[4] : V - 1;
+  g->last_forest_edges = st[4] < g->V ? st[4] : g->V - 1;
   g->labels_valid = true;
   g->labels_level = level;
   return GS_OK;
+}
+
+gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s) {
+  GS_TRY(gs_boruvka_enqueue(g, level, round0_col, s, g->h_status));
+  GS_CUDA_TRY(cudaStreamSynchronize(s));
+  return gs_boruvka_finish(g, level, g->h_status);
 }

@@ -23,9 +23,12 @@ void gs_free_graph(gs_graph* g) {
   if (!g) return;
   cudaFree(g->d_sk); cudaFree(g->d_colmix);
   cudaFree(g->d_cnt); cudaFree(g->d_off); cudaFree(g->d_choff); cudaFree(g->d_tile);
-  cudaFree(g->d_nbr); cudaFree(g->d_pairs); cudaFree(g->d_part); cudaFree(g->d_bkt);
+  cudaFree(g->d_nbr); cudaFree(g->d_pairs); cudaFree(g->d_file_pairs); cudaFree(g->d_part); cudaFree(g->d_bkt);
   if (g->h_pin) cudaFreeHost(g->h_pin);
   if (g->h_status) cudaFreeHost(g->h_status);
+  if (g->h_qstatus) cudaFreeHost(g->h_qstatus);
+  if (g->h_qlabels) cudaFreeHost(g->h_qlabels);
+  if (g->ev_query) cudaEventDestroy(g->ev_query);
   cudaFree(g->d_status);
   cudaFree(g->d_parent); cudaFree(g->d_size); cudaFree(g->d_res); cudaFree(g->d_samp); cudaFree(g->d_acc);
   cudaFree(g->d_forest);
@@ -155,9 +158,9 @@ gs_status gs_graph_create(const gs_graph_config* cfg, gs_graph** out) {
   colmix[C] = gs_seed_mix(g->seed);                                                 // checksum_seed (sketch.h:304)
   GS_CUDA_TRY(cudaMalloc(&g->d_colmix, (C + 1) * sizeof(uint64_t)));
   GS_CUDA_TRY(cudaMemcpy(g->d_colmix, colmix.data(), (C + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice));
-  GS_CUDA_TRY(cudaMalloc(&g->d_status, 16 * sizeof(uint32_t)));
-  GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 16 * sizeof(uint32_t), g->stream));
-  GS_CUDA_TRY(cudaMallocHost(&g->h_status, 16 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMalloc(&g->d_status, 32 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 32 * sizeof(uint32_t), g->stream));
+  GS_CUDA_TRY(cudaMallocHost(&g->h_status, 32 * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMalloc(&g->d_parent, (size_t)V * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMalloc(&g->d_size, (size_t)V * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMalloc(&g->d_res, (size_t)V * sizeof(uint32_t)));
@@ -195,6 +198,7 @@ gs_status gs_clear(gs_graph* g) {
   const size_t bytes = (size_t)g->num_levels * g->V * g->geom.num_buckets * sizeof(GsBucket);
   GS_CUDA_TRY(cudaMemsetAsync(g->d_sk, 0, bytes, g->stream));
   g->labels_valid = false;
+  g->changes++;
   std::fill(g->sample_cursor.begin(), g->sample_cursor.end(), 0u);
   GS_TRY(gs_store_clear(g, g->stream));
   return gs_eager_reset_empty(g, g->stream);
@@ -214,19 +218,17 @@ uint64_t gs_desired_updates_per_batch(const gs_graph* g) {
   return (uint64_t)(n * g->batch_factor);
 }
 
-gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int on_device, void* stream) {
-  if (!g || (n && !pairs)) { gs_set_error("gs_ingest_pairs: null argument"); return GS_ERR_BAD_ARG; }
-  if (n == 0) return GS_OK;
-  GS_GUARD(g);
-  cudaStream_t s = pick_stream(g, stream);
-  g->labels_valid = false;
-  if (on_device) {
-    GS_TRY(gs_ingest_device_pairs(g, pairs, n, -1, s));
-    return order_after(g, s);
-  }
+}  // extern "C"
 
-  // host input: double-buffered H2D through the pinned ring (or straight from caller memory that
-  // is already page-locked), overlapped with the ingest of the previous slice
+namespace {
+
+// Host input moves through the staging slots: slice k is copied on the copy stream into device slot
+// k % 2 (from the caller's memory when it is page-locked, else through the pinned ring) while the
+// ingest of slice k - 1 runs.  With `wait_copies`, the call returns once every copy has landed (the
+// caller may reuse its buffer); without, it returns at once for page-locked input, whose buffer then
+// stays in use until the handle's work is done, and every wait on a slot's earlier slice happens on
+// the device, so copies of this call can run ahead of queries queued before it.
+gs_status ingest_host_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, cudaStream_t s, bool wait_copies) {
   GS_TRY(gs_ensure_pair_staging(g));
   cudaPointerAttributes attr{};
   const bool pinned = cudaPointerGetAttributes(&attr, pairs) == cudaSuccess && attr.type == cudaMemoryTypeHost;
@@ -237,13 +239,17 @@ gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int on
     const uint64_t m = std::min(cap, n - done);
     const int slot = (int)(k & 1);
     uint32_t* dslot = g->d_pairs + (size_t)slot * cap * 2;
-    // slice k-2 (same slot) must be consumed before its device and pinned buffers are reused
-    GS_CUDA_TRY(cudaEventSynchronize(g->ev_done[slot]));
     const uint32_t* src = pairs + 2 * done;
     if (!pinned) {
+      // the pinned slot is free once its previous copy has landed; the device slot once the ingest that
+      // read it has finished
+      GS_CUDA_TRY(cudaEventSynchronize(wait_copies ? g->ev_done[slot] : g->ev_copy[slot]));
       std::memcpy(hp + (size_t)slot * cap * 2, src, (size_t)m * 2 * sizeof(uint32_t));
       src = hp + (size_t)slot * cap * 2;
+    } else if (wait_copies) {
+      GS_CUDA_TRY(cudaEventSynchronize(g->ev_done[slot]));
     }
+    GS_CUDA_TRY(cudaStreamWaitEvent(g->copy_stream, g->ev_done[slot], 0));
     GS_CUDA_TRY(cudaMemcpyAsync(dslot, src, (size_t)m * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice,
                                 g->copy_stream));
     GS_CUDA_TRY(cudaEventRecord(g->ev_copy[slot], g->copy_stream));
@@ -253,8 +259,92 @@ gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int on
     done += m;
   }
   // the caller's buffer may be reused once every copy has landed
-  GS_CUDA_TRY(cudaStreamSynchronize(g->copy_stream));
+  if (wait_copies) GS_CUDA_TRY(cudaStreamSynchronize(g->copy_stream));
   return order_after(g, s);
+}
+
+constexpr uint64_t al16(uint64_t x) { return (x + 15) & ~15ull; }
+
+// Host per-vertex batches move through the same staging slots as host pairs, so a call allocates
+// nothing: the batches are cut into chunks that fit one slot (a batch longer than the room left is
+// split; XOR makes the pieces equivalent to the whole), each chunk's headers and destinations are
+// gathered into the slot's page-locked half - starts rebased to the gathered destinations - copied to
+// the device half and ingested while the next chunk is gathered.
+gs_status ingest_host_batches(gs_graph* g, uint32_t level, const uint32_t* srcs, const uint64_t* starts,
+                              const uint64_t* sizes, uint32_t nbat, const uint32_t* dsts, cudaStream_t s) {
+  GS_TRY(gs_ensure_pair_staging(g));
+  const uint64_t slot_bytes = g->pairs_cap * 2 * sizeof(uint32_t);
+  // a slot: batch headers (srcs u32, starts u64, sizes u64) in its first quarter, destinations after
+  const uint64_t hb = std::max<uint64_t>(1, (slot_bytes / 4) / 24);
+  const uint64_t off_starts = al16(hb * 4), off_sizes = off_starts + al16(hb * 8);
+  const uint64_t off_dsts = al16(off_sizes + hb * 8);
+  const uint64_t dcap = (slot_bytes - off_dsts) / sizeof(uint32_t);
+  uint8_t* hp = static_cast<uint8_t*>(g->h_pin);
+  uint8_t* dp = reinterpret_cast<uint8_t*>(g->d_pairs);
+  uint32_t b = 0;
+  uint64_t in_batch = 0;  // destinations of batch b already shipped
+  for (int k = 0; b < nbat; k++) {
+    const int slot = k & 1;
+    GS_CUDA_TRY(cudaEventSynchronize(g->ev_done[slot]));   // the slot's previous chunk was ingested
+    uint8_t* h = hp + slot * slot_bytes;
+    uint32_t* hs = reinterpret_cast<uint32_t*>(h);
+    uint64_t* hst = reinterpret_cast<uint64_t*>(h + off_starts);
+    uint64_t* hsz = reinterpret_cast<uint64_t*>(h + off_sizes);
+    uint32_t* hd = reinterpret_cast<uint32_t*>(h + off_dsts);
+    uint64_t nb = 0, nd = 0;
+    while (b < nbat && nb < hb && nd < dcap) {
+      const uint64_t take = std::min(sizes[b] - in_batch, dcap - nd);
+      hs[nb] = srcs[b];
+      hst[nb] = nd;
+      hsz[nb] = take;
+      std::memcpy(hd + nd, dsts + starts[b] + in_batch, take * sizeof(uint32_t));
+      nb++;
+      nd += take;
+      in_batch += take;
+      if (in_batch == sizes[b]) { b++; in_batch = 0; }
+    }
+    uint8_t* d = dp + slot * slot_bytes;
+    GS_CUDA_TRY(cudaMemcpyAsync(d, h, off_sizes + nb * 8, cudaMemcpyHostToDevice, s));
+    if (nd) GS_CUDA_TRY(cudaMemcpyAsync(d + off_dsts, hd, nd * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    GS_TRY(gs_ingest_device_batches(g, level, reinterpret_cast<const uint32_t*>(d),
+                                    reinterpret_cast<const uint64_t*>(d + off_starts),
+                                    reinterpret_cast<const uint64_t*>(d + off_sizes), (uint32_t)nb,
+                                    reinterpret_cast<const uint32_t*>(d + off_dsts), s));
+    GS_CUDA_TRY(cudaEventRecord(g->ev_done[slot], s));
+  }
+  return order_after(g, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int on_device, void* stream) {
+  if (!g || (n && !pairs)) { gs_set_error("gs_ingest_pairs: null argument"); return GS_ERR_BAD_ARG; }
+  if (n == 0) return GS_OK;
+  GS_GUARD(g);
+  cudaStream_t s = pick_stream(g, stream);
+  g->labels_valid = false;
+  g->changes++;
+  if (on_device) {
+    GS_TRY(gs_ingest_device_pairs(g, pairs, n, -1, s));
+    return order_after(g, s);
+  }
+  return ingest_host_pairs(g, pairs, n, s, true);
+}
+
+gs_status gs_ingest_pairs_async(gs_graph* g, const uint32_t* pairs, uint64_t n, int on_device, void* stream) {
+  if (!g || (n && !pairs)) { gs_set_error("gs_ingest_pairs_async: null argument"); return GS_ERR_BAD_ARG; }
+  if (n == 0) return GS_OK;
+  GS_GUARD(g);
+  cudaStream_t s = pick_stream(g, stream);
+  g->labels_valid = false;
+  g->changes++;
+  if (on_device) {
+    GS_TRY(gs_ingest_device_pairs(g, pairs, n, -1, s));
+    return order_after(g, s);
+  }
+  return ingest_host_pairs(g, pairs, n, s, false);
 }
 
 gs_status gs_ingest_edges(gs_graph* g, const uint32_t* src, const uint32_t* dst, uint64_t n, int on_device,
@@ -270,6 +360,7 @@ gs_status gs_ingest_edges(gs_graph* g, const uint32_t* src, const uint32_t* dst,
   // device arrays: interleaved on the device into the staging slots, one slice at a time
   cudaStream_t s = pick_stream(g, stream);
   g->labels_valid = false;
+  g->changes++;
   GS_TRY(gs_ensure_pair_staging(g));
   const uint64_t cap = g->pairs_cap;
   for (uint64_t done = 0, k = 0; done < n; k++) {
@@ -300,6 +391,7 @@ gs_status gs_ingest_vertex_batches(gs_graph* g, uint32_t level, const uint32_t* 
   GS_GUARD(g);
   cudaStream_t s = pick_stream(g, stream);
   g->labels_valid = false;
+  g->changes++;
   if (on_device) {
     GS_TRY(gs_ingest_device_batches(g, level, srcs, starts, sizes, nbat, dsts, s));
     return order_after(g, s);
@@ -310,28 +402,7 @@ gs_status gs_ingest_vertex_batches(gs_graph* g, uint32_t level, const uint32_t* 
       return GS_ERR_BAD_ARG;
     }
   }
-  uint32_t *d_srcs = nullptr, *d_dsts = nullptr;
-  uint64_t *d_starts = nullptr, *d_sizes = nullptr;
-  gs_status st = GS_OK;
-  auto fail = [&](cudaError_t e) {
-    gs_set_error(std::string("gs_ingest_vertex_batches: ") + cudaGetErrorString(e));
-    st = e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA;
-  };
-  cudaError_t e;
-  if ((e = cudaMalloc(&d_srcs, nbat * sizeof(uint32_t))) != cudaSuccess) fail(e);
-  else if ((e = cudaMalloc(&d_starts, nbat * sizeof(uint64_t))) != cudaSuccess) fail(e);
-  else if ((e = cudaMalloc(&d_sizes, nbat * sizeof(uint64_t))) != cudaSuccess) fail(e);
-  else if ((e = cudaMalloc(&d_dsts, std::max<uint64_t>(ndst, 1) * sizeof(uint32_t))) != cudaSuccess) fail(e);
-  if (st == GS_OK) {
-    cudaMemcpyAsync(d_srcs, srcs, nbat * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_starts, starts, nbat * sizeof(uint64_t), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_sizes, sizes, nbat * sizeof(uint64_t), cudaMemcpyHostToDevice, s);
-    if (ndst) cudaMemcpyAsync(d_dsts, dsts, ndst * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
-    st = gs_ingest_device_batches(g, level, d_srcs, d_starts, d_sizes, nbat, d_dsts, s);
-    cudaStreamSynchronize(s);
-  }
-  cudaFree(d_srcs); cudaFree(d_starts); cudaFree(d_sizes); cudaFree(d_dsts);
-  return st;
+  return ingest_host_batches(g, level, srcs, starts, sizes, nbat, dsts, s);
 }
 
 gs_status gs_synchronize(gs_graph* g) {
@@ -344,6 +415,7 @@ gs_status gs_synchronize(gs_graph* g) {
 gs_status gs_connected_components(gs_graph* g, uint32_t level, uint32_t* labels, uint32_t* num_cc, uint32_t* rounds) {
   if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
   if (level >= g->num_levels) { gs_set_error("level out of range"); return GS_ERR_BAD_ARG; }
+  if (g->query_pending) { gs_set_error("a queued query is pending: collect it with gs_query_wait first"); return GS_ERR_BAD_ARG; }
   GS_GUARD(g);
   cudaStream_t s = g->stream;
   GS_TRY(check_status(g, s));
@@ -368,6 +440,79 @@ gs_status gs_connected_components(gs_graph* g, uint32_t level, uint32_t* labels,
       for (uint32_t v = 0; v < g->V; v++) c += dst[v] == v;
       *num_cc = c;
     }
+  }
+  return GS_OK;
+}
+
+gs_status gs_connected_components_async(gs_graph* g, uint32_t level) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  if (level >= g->num_levels) { gs_set_error("level out of range"); return GS_ERR_BAD_ARG; }
+  if (g->query_pending) { gs_set_error("a queued query is pending: collect it with gs_query_wait first"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  cudaStream_t s = g->stream;
+  if (!g->h_qlabels) {
+    GS_CUDA_TRY(cudaMallocHost(&g->h_qstatus, 32 * sizeof(uint32_t)));
+    GS_CUDA_TRY(cudaMallocHost(&g->h_qlabels, (size_t)g->V * sizeof(uint32_t)));
+    GS_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_query, cudaEventDisableTiming));
+  }
+  g->query_level = level;
+  g->query_changes = g->changes;
+  g->query_done = false;
+  g->query_status = GS_OK;
+  if (level == 0 && g->eager_on) {
+    // the eager DSU answers at once (it synchronizes anyway); gs_query_wait hands the answer out
+    uint32_t ncc = 0, rounds = 0;
+    g->query_status = gs_connected_components(g, 0, g->h_qlabels, &ncc, &rounds);
+    g->h_qstatus[0] = ncc;
+    g->h_qstatus[1] = rounds;
+    g->query_done = true;
+    g->query_pending = true;
+    return GS_OK;
+  }
+  GS_TRY(gs_boruvka_enqueue(g, level, 0, s, g->h_qstatus));
+  GS_CUDA_TRY(cudaMemcpyAsync(g->h_qlabels, g->d_parent, (size_t)g->V * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GS_CUDA_TRY(cudaEventRecord(g->ev_query, s));
+  g->query_pending = true;
+  return GS_OK;
+}
+
+gs_status gs_query_wait(gs_graph* g, uint32_t* labels, uint32_t* num_cc, uint32_t* rounds) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  if (!g->query_pending) { gs_set_error("gs_query_wait: no query is queued"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  g->query_pending = false;
+  const uint32_t V = g->V;
+  if (g->query_done) {
+    if (g->query_status != GS_OK) return g->query_status;
+    if (labels) std::memcpy(labels, g->h_qlabels, (size_t)V * sizeof(uint32_t));
+    if (num_cc) *num_cc = g->h_qstatus[0];
+    if (rounds) *rounds = g->h_qstatus[1];
+    return GS_OK;
+  }
+  GS_CUDA_TRY(cudaEventSynchronize(g->ev_query));
+  const uint32_t* st = g->h_qstatus;
+  if (st[16] & GS_DEV_ERR_VERTEX_RANGE) {
+    // as gs_connected_components, which reports records skipped by earlier ingest calls first
+    gs_set_error("an edge record named a vertex id >= num_vertices; those records were skipped");
+    g->acc_dirty = true;
+    return GS_ERR_BAD_ARG;
+  }
+  if (st[16]) {
+    gs_set_error("device consistency check failed (bits " + std::to_string(st[16]) + ")");
+    g->acc_dirty = true;
+    return GS_ERR_INTERNAL;
+  }
+  GS_TRY(gs_boruvka_finish(g, g->query_level, st));
+  g->last_answer_eager = false;
+  // the partition stays valid for point queries only while no later call has changed the sketches
+  g->labels_valid = g->changes == g->query_changes;
+  if (g->query_level == 0 && g->eager_on) GS_TRY(gs_eager_rebuild(g, g->stream));
+  if (rounds) *rounds = g->last_rounds;
+  if (labels) std::memcpy(labels, g->h_qlabels, (size_t)V * sizeof(uint32_t));
+  if (num_cc) {
+    uint32_t c = 0;
+    for (uint32_t v = 0; v < V; v++) c += g->h_qlabels[v] == v;
+    *num_cc = c;
   }
   return GS_OK;
 }
@@ -397,6 +542,7 @@ gs_status gs_spanning_forest(gs_graph* g, uint32_t level, uint32_t* edges, uint6
 
 gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, uint32_t* edges, uint64_t* sizes) {
   if (!g || !edges || !sizes || k == 0) { gs_set_error("gs_disjoint_spanning_forests: bad arguments"); return GS_ERR_BAD_ARG; }
+  if (g->query_pending) { gs_set_error("a queued query is pending: collect it with gs_query_wait first"); return GS_ERR_BAD_ARG; }
   if (level >= g->num_levels) { gs_set_error("level out of range"); return GS_ERR_BAD_ARG; }
   GS_GUARD(g);
   cudaStream_t s = g->stream;
@@ -430,6 +576,7 @@ gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, 
   cudaFree(d_all);
   for (uint32_t j = done; j < k; j++) sizes[j] = 0;
   g->labels_valid = false;
+  g->changes++;
   gs_eager_invalidate(g, s);  // the parent array now holds the last forest's partition
   if (st != GS_OK) return st;
   if (st2 != GS_OK) return st2;
@@ -515,6 +662,7 @@ gs_status gs_upload_sketches(gs_graph* g, uint32_t level, uint32_t first, uint32
   GS_CUDA_TRY(cudaMemcpy(g->d_sk + ((size_t)level * g->V + first) * nb, host_in, (size_t)count * nb * sizeof(GsBucket),
                          cudaMemcpyHostToDevice));
   g->labels_valid = false;
+  g->changes++;
   return gs_eager_invalidate(g, g->stream);
 }
 

@@ -463,9 +463,9 @@ gs_status gs_engine_create(const gs_engine_config* cfg, gs_engine** out) {
   }
   const uint32_t T1 = e->max_tenants + 1;
   GS_CUDA_TRY(cudaMalloc(&g->d_colmix, (size_t)T1 * kColStride * sizeof(uint64_t)));
-  GS_CUDA_TRY(cudaMalloc(&g->d_status, 16 * sizeof(uint32_t)));
-  GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 16 * sizeof(uint32_t), g->stream));
-  GS_CUDA_TRY(cudaMallocHost(&g->h_status, 16 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMalloc(&g->d_status, 32 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, 32 * sizeof(uint32_t), g->stream));
+  GS_CUDA_TRY(cudaMallocHost(&g->h_status, 32 * sizeof(uint32_t)));
   const size_t V = e->max_vertices;
   GS_CUDA_TRY(cudaMalloc(&g->d_parent, V * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMalloc(&g->d_size, V * sizeof(uint32_t)));

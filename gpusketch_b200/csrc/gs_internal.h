@@ -86,11 +86,24 @@ struct gs_graph {
   uint32_t* d_pairs = nullptr; // staging for host-resident input pairs, 2 x [pairs_cap] u32 pairs
   uint64_t pairs_cap = 0;
   void* h_pin = nullptr;       // 2 pinned staging buffers of pairs_cap pairs
+  uint2* d_file_pairs = nullptr; // decoded records of one stream-file slice (gs_ingest_stream_file)
   cudaStream_t copy_stream = nullptr;               // H2D of host input slices
   cudaEvent_t ev_copy[2] = {nullptr, nullptr};      // slice copied into d_pairs[slot]
   cudaEvent_t ev_done[2] = {nullptr, nullptr};      // slice in d_pairs[slot] consumed
   uint32_t* d_status = nullptr;  // [0] error bits [1] records [2] chunks [3] modified [4] forest [5] part chunks
-  uint32_t* h_status = nullptr;  // pinned mirror
+                                 // ... [16] ingest error bits carried across a query (32 words)
+  uint32_t* h_status = nullptr;  // pinned mirror (32 words)
+  uint64_t changes = 0;          // count of calls that changed the sketches
+
+  // ---- asynchronous query (gs_connected_components_async / gs_query_wait) ----
+  bool query_pending = false;
+  uint32_t query_level = 0;
+  uint64_t query_changes = 0;      // `changes` when the query was queued
+  gs_status query_status = GS_OK;  // answer already known at submission (eager DSU, or an error)
+  bool query_done = false;
+  uint32_t* h_qstatus = nullptr;   // pinned, 32 words: the query's status words
+  uint32_t* h_qlabels = nullptr;   // pinned, V labels
+  cudaEvent_t ev_query = nullptr;  // recorded after the labels' read-back
 
   // ---- Boruvka scratch ----
   uint32_t* d_parent = nullptr;  // [V]
@@ -179,6 +192,11 @@ gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* 
                                    uint32_t nb, const uint32_t* d_dsts, cudaStream_t s);
 // Device Boruvka on one level; forest edges stay in g->d_forest.
 gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s);
+// The same in two halves: the launch and the read-back of status words [0, 17) into pinned h_out
+// (word 16: ingest error bits queued before the query), queued on s without waiting; then, once
+// that work is done, the interpretation of those words.
+gs_status gs_boruvka_enqueue(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s, uint32_t* h_out);
+gs_status gs_boruvka_finish(gs_graph* g, uint32_t level, const uint32_t* st);
 
 // Eager DSU (gs_eager.cu).
 gs_status gs_eager_enable(gs_graph* g, bool on, cudaStream_t s);

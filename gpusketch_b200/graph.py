@@ -144,6 +144,25 @@ class GraphSketch:
         check(self._lib.gs_ingest_pairs(self._h, p, n, int(dev), _device_stream(stream, dev)), "gs_ingest_pairs")
         del keep
 
+    def ingest_pairs_async(self, pairs, stream=None) -> None:
+        """gs_ingest_pairs_async: queue the copies and the ingest without waiting.  A page-locked host
+        buffer (a pinned CPU tensor) stays in use until the handle's queued work is done: keep it alive
+        and unchanged until synchronize(), query_wait() or a synchronous query."""
+        p, n, dev, keep = _as_pairs(pairs)
+        if keep is not pairs and not dev:
+            raise ValueError("ingest_pairs_async needs a C-contiguous uint32/int32 buffer the caller keeps alive")
+        check(self._lib.gs_ingest_pairs_async(self._h, p, n, int(dev), _device_stream(stream, dev)),
+              "gs_ingest_pairs_async")
+
+    def ingest_stream_file(self, path: str, first: int = 0, count: int | None = None) -> int:
+        """gs_ingest_stream_file: records [first, first+count) of a binary stream file; returns the number
+        of records ingested."""
+        n = C.c_uint64()
+        check(self._lib.gs_ingest_stream_file(self._h, str(path).encode(), first,
+                                              2**64 - 1 if count is None else count, C.byref(n)),
+              "gs_ingest_stream_file")
+        return n.value
+
     def ingest_edges(self, src, dst, stream=None) -> None:
         """gs_ingest_edges: record i toggles edge {src[i], dst[i]}; both arrays on the host or both on
         the device."""
@@ -173,6 +192,17 @@ class GraphSketch:
         ncc, rounds = C.c_uint32(), C.c_uint32()
         check(self._lib.gs_connected_components(self._h, level, labels.ctypes.data, C.byref(ncc), C.byref(rounds)),
               "gs_connected_components")
+        return labels, ncc.value, rounds.value
+
+    def connected_components_async(self, level: int = 0) -> None:
+        """Queue connected_components(level); collect the answer with query_wait()."""
+        check(self._lib.gs_connected_components_async(self._h, level), "gs_connected_components_async")
+
+    def query_wait(self):
+        """(labels, num_cc, rounds) of the query queued by connected_components_async()."""
+        labels = np.empty(self.num_vertices, np.uint32)
+        ncc, rounds = C.c_uint32(), C.c_uint32()
+        check(self._lib.gs_query_wait(self._h, labels.ctypes.data, C.byref(ncc), C.byref(rounds)), "gs_query_wait")
         return labels, ncc.value, rounds.value
 
     def point_query(self, a: int, b: int) -> bool:

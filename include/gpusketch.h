@@ -121,6 +121,30 @@ uint64_t gs_desired_updates_per_batch(const gs_graph* g);
 gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int pairs_on_device,
                           void* cuda_stream);
 
+/* gs_ingest_pairs without waiting for host input to be copied: the call queues the copies and the
+ * ingest and returns.  For page-locked host memory it returns at once and the buffer stays in use until
+ * the handle's queued work is done (gs_synchronize, gs_query_wait, or any synchronous query): the caller
+ * must neither free nor change it before then.  Pageable memory is still staged through the pinned
+ * ring and may be reused when the call returns.  The copies wait for their staging slots on the
+ * device, so copies of the next phase's records proceed while a query queued with
+ * gs_connected_components_async runs.  Device input behaves as in gs_ingest_pairs.  Library extension
+ * (the reference's CudaStream waits for each buffer, include/cuda_stream.h:146-202). */
+gs_status gs_ingest_pairs_async(gs_graph* g, const uint32_t* pairs, uint64_t n, int pairs_on_device,
+                                void* cuda_stream);
+
+/* Edge records [first, first+count) of a binary stream file in the reference's format (a header
+ * {u32 num_vertices, u64 num_updates}, then packed 9-byte records {u8 type, u32 src, u32 dst}; the
+ * StreamingUtilities BinaryFileStream read by the reference's tools and tests).  count may exceed the
+ * records left (UINT64_MAX: to the end).  The file is read in slices by several threads straight into
+ * the library's page-locked ring, copied to the device as raw records and decoded there; the read and
+ * copy of slice k+1 overlap the ingest of slice k.  Every record toggles its edge whatever its type
+ * byte, as in the reference's sketch update.  *ingested (may be NULL) receives the record count.
+ * GS_ERR_IO on an unreadable or truncated file, GS_ERR_BAD_ARG when the file's vertex count exceeds
+ * the graph's.  Replaces the reader threads of GraphSketchDriver::process_stream_until
+ * (include/graph_sketch_driver.h:141-191) for file streams. */
+gs_status gs_ingest_stream_file(gs_graph* g, const char* path, uint64_t first, uint64_t count,
+                                uint64_t* ingested);
+
 /* Same as gs_ingest_pairs with separate src / dst arrays (device arrays are interleaved on the device). */
 gs_status gs_ingest_edges(gs_graph* g, const uint32_t* src, const uint32_t* dst, uint64_t n,
                           int on_device, void* cuda_stream);
@@ -144,6 +168,18 @@ gs_status gs_synchronize(gs_graph* g);
  * GS_ERR_SKETCH_FAIL when the sketch runs out of columns. */
 gs_status gs_connected_components(gs_graph* g, uint32_t level, uint32_t* labels, uint32_t* num_cc,
                                   uint32_t* rounds);
+
+/* connected_components() queued without waiting for it (library extension): the query sees every
+ * update queued before it and none queued after it, so the caller can queue the next phase's ingest
+ * (gs_ingest_pairs_async) while it runs.  gs_query_wait collects the answer; until then no other query
+ * may be made on the handle (GS_ERR_BAD_ARG).  The first call allocates page-locked space for the
+ * answer (V labels).  With the eager DSU on, the answer is computed at once. */
+gs_status gs_connected_components_async(gs_graph* g, uint32_t level);
+/* Waits for the query queued by gs_connected_components_async and returns what gs_connected_components
+ * would have returned for it: labels (host, length V, may be NULL), num_cc and rounds (may be NULL),
+ * GS_ERR_SKETCH_FAIL when the sketches ran out of columns, GS_ERR_BAD_ARG when an ingest queued before
+ * the query had skipped out-of-range records. */
+gs_status gs_query_wait(gs_graph* g, uint32_t* labels, uint32_t* num_cc, uint32_t* rounds);
 
 /* CCSketchAlg::point_query (src/cc_sketch_alg.cpp:630-672). */
 gs_status gs_point_query(gs_graph* g, uint32_t a, uint32_t b, int* connected);

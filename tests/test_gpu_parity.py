@@ -459,3 +459,42 @@ def test_min_cut_falls_back_to_the_exact_tier():
         exact = g.edge_store_edges(1)
         lam, _ = gs.exact_min_cut(V, exact)
         assert cut_at == lam
+
+
+@pytest.mark.parametrize("pinned", [True, False])
+def test_async_ingest_and_query_overlap_phases(restatement, pinned):
+    """gs_ingest_pairs_async + gs_connected_components_async: the next phase's records are queued
+    (copies included) while the previous phase's query runs; every answer equals the exact partition of
+    its own prefix, and the final sketches equal the oracle's, from page-locked and pageable input in
+    several staging slices."""
+    import torch
+    V, seed, P = 6000, 0x5EED3400, 4
+    rng = np.random.default_rng(34)
+    pairs = rng.integers(0, V, size=(P * 70_001, 2), dtype=np.uint32)
+    pairs = pairs[(pairs[:, 0] % 4) == (pairs[:, 1] % 4)]            # several components
+    bounds = np.linspace(0, len(pairs), P + 1).astype(int)
+    host = torch.from_numpy(pairs.view(np.int32)).pin_memory() if pinned else pairs
+    with gs.GraphSketch(V, seed, max_batch_edges=1 << 14) as g:
+        answers = []
+        g.ingest_pairs_async(host[bounds[0]:bounds[1]])
+        for p in range(P):
+            g.connected_components_async()
+            with pytest.raises(gs.GpuSketchError):
+                g.connected_components_async()                   # one queued query at a time
+            with pytest.raises(gs.GpuSketchError):
+                g.connected_components()
+            if p + 1 < P:
+                g.ingest_pairs_async(host[bounds[p + 1]:bounds[p + 2]])   # queued behind the query
+            answers.append(g.query_wait())
+        for p, (labels, ncc, rounds) in enumerate(answers):
+            n, exact = restatement.exact_cc(V, pairs[:bounds[p + 1]])
+            assert ncc == n and np.array_equal(labels, exact), p
+        g.synchronize()
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, pairs)
+        # a later ingest makes the queued answer stale for point queries
+        g.ingest_pairs(np.array([[1, 2]], np.uint32))
+        want = restatement.exact_cc(V, np.concatenate([pairs, [[1, 2]]]).astype(np.uint32))[1]
+        assert g.point_query(1, 2) == (want[1] == want[2]) == True
+    with pytest.raises(gs.GpuSketchError):
+        with gs.GraphSketch(V, seed) as g2:
+            g2.query_wait()                                      # nothing queued
