@@ -76,6 +76,8 @@ SIGNATURES = {
     "gs_query_wait": (C.c_int, [_P, _P, _U32P, _U32P]),
     "gs_ingest_vertex_batches": (C.c_int, [_P, C.c_uint32, _P, _P, _P, C.c_uint32, _P, C.c_uint64, C.c_int, _P]),
     "gs_synchronize": (C.c_int, [_P]),
+    "gs_graph_set_edge_store": (C.c_int, [_P, C.c_uint32, C.c_uint64]),
+    "gs_graph_sketched_levels": (C.c_int, [_P, _U32P, _U64P]),
     "gs_set_device_wait_limit": (C.c_int, [_P, C.c_uint64]),
     "gs_connected_components": (C.c_int, [_P, C.c_uint32, _P, _U32P, _U32P]),
     "gs_point_query": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(C.c_int)]),

@@ -33,6 +33,7 @@ void gs_free_graph(gs_graph* g) {
   cudaFree(g->d_parent); cudaFree(g->d_size); cudaFree(g->d_res); cudaFree(g->d_samp); cudaFree(g->d_acc);
   cudaFree(g->d_forest);
   cudaFree(g->d_store);
+  cudaFree(g->d_store_list);
   cudaFree(g->d_store_status);
   if (g->h_store) cudaFreeHost(g->h_store);
   cudaFree(g->d_eager_set);
@@ -140,6 +141,7 @@ gs_status gs_graph_create(const gs_graph_config* cfg, gs_graph** out) {
   g->device = dev;
   g->max_batch_edges = cfg->max_batch_edges ? cfg->max_batch_edges : (1ull << 27);
   if (g->max_batch_edges > (1ull << 30)) g->max_batch_edges = 1ull << 30;
+  g->store_first = g->store_initial = g->num_levels;
   g->geom = gs_make_geom(g->V, g->sketches_factor);
   if (g->geom.num_columns > 64) { gs_set_error("more than 64 sketch columns are not supported"); return GS_ERR_BAD_ARG; }
   cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -200,6 +202,8 @@ gs_status gs_clear(gs_graph* g) {
   g->labels_valid = false;
   g->changes++;
   std::fill(g->sample_cursor.begin(), g->sample_cursor.end(), 0u);
+  g->store_first = g->store_initial;
+  g->changes_at_clear = g->changes;
   GS_TRY(gs_store_clear(g, g->stream));
   return gs_eager_reset_empty(g, g->stream);
 }
@@ -557,7 +561,7 @@ gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, 
   for (uint32_t j = 0; j < k; j++) {
     // a min-cut graph samples round 0 at the column its stored sample index reached; a
     // connected-components graph resets it before every query (CCSketchAlg::connected_components)
-    const uint32_t col0 = g->num_levels > 1 ? g->sample_cursor[level]++ : 0;
+    const uint32_t col0 = (g->num_levels > 1 || g->num_subgraphs > 1) ? g->sample_cursor[level]++ : 0;
     st = gs_boruvka(g, level, col0, s);
     if (st != GS_OK) break;
     const uint32_t ne = g->last_forest_edges;
@@ -590,14 +594,16 @@ gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_f
   const uint32_t V = g->V;
   std::vector<uint32_t> edges((size_t)k * 2 * (V - 1));
   std::vector<uint64_t> sizes(k);
-  for (uint32_t lvl = 0; lvl < g->num_levels; lvl++) {
+  // the levels sketched now (all configured levels unless the exact tier is adaptive)
+  const uint32_t sketched = g->store_first;
+  for (uint32_t lvl = 0; lvl < sketched; lvl++) {
     GS_TRY(gs_disjoint_spanning_forests(g, lvl, k, edges.data(), sizes.data()));
     std::vector<uint32_t> cert;
     for (uint32_t f = 0; f < k; f++)
       cert.insert(cert.end(), edges.begin() + (size_t)f * 2 * (V - 1),
                   edges.begin() + (size_t)f * 2 * (V - 1) + 2 * sizes[f]);
     const uint64_t cut = gs_exact_min_cut_host(V, cert.data(), cert.size() / 2, side);
-    if (cut < k || (lvl + 1 == g->num_levels && !gs_store_active(g))) {
+    if (cut < k || (lvl + 1 == sketched && !gs_store_active(g))) {
       *value = cut << lvl;
       if (level_found) *level_found = lvl;
       if (cut_at_level) *cut_at_level = cut;
@@ -607,7 +613,7 @@ gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_f
   // no sketched level certified a cut below k: the first unsketched level answers whatever its
   // value, with the exact minimum cut of all its edges from the exact tier (tools/min_cut.cu:221-247;
   // get_adjlist_spanning_forests returns the store's whole edge list, src/mc_gpu_sketch_alg.cpp:207-209)
-  const uint32_t lvl = g->num_levels;
+  const uint32_t lvl = sketched;
   {
     GS_GUARD(g);
     GS_TRY(check_status(g, g->stream));
@@ -618,6 +624,35 @@ gs_status gs_min_cut(gs_graph* g, uint32_t k, uint64_t* value, uint32_t* level_f
     if (level_found) *level_found = lvl;
     if (cut_at_level) *cut_at_level = cut;
   }
+  return GS_OK;
+}
+
+gs_status gs_graph_set_edge_store(gs_graph* g, uint32_t initial_sketch_levels, uint64_t store_bytes) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  if (initial_sketch_levels > g->num_levels || g->num_subgraphs <= 1) {
+    gs_set_error("gs_graph_set_edge_store: a min-cut graph (num_subgraphs > 1) and initial_sketch_levels <= num_levels");
+    return GS_ERR_BAD_ARG;
+  }
+  if (g->changes != g->changes_at_clear) {
+    gs_set_error("gs_graph_set_edge_store: set the exact tier before the first ingest (or right after gs_clear)");
+    return GS_ERR_BAD_ARG;
+  }
+  GS_GUARD(g);
+  const uint64_t level_bytes = (uint64_t)g->V * g->geom.num_buckets * sizeof(GsBucket);
+  g->store_initial = g->store_first = initial_sketch_levels;
+  g->store_adaptive = true;
+  g->store_budget = std::max<uint64_t>(1, (store_bytes ? store_bytes : level_bytes) / 16);
+  if (g->d_store) {   // sized for the default budget: the next tagged ingest sizes it again
+    cudaFree(g->d_store);
+    g->d_store = nullptr;
+  }
+  return GS_OK;
+}
+
+gs_status gs_graph_sketched_levels(const gs_graph* g, uint32_t* levels, uint64_t* contractions) {
+  if (!g || !levels) { gs_set_error("null argument"); return GS_ERR_BAD_ARG; }
+  *levels = g->store_first;
+  if (contractions) *contractions = g->store_contractions;
   return GS_OK;
 }
 

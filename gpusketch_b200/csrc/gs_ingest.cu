@@ -1201,13 +1201,23 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
                                  cudaStream_t s) {
   if (n == 0) return GS_OK;
   const uint32_t nv = g->num_levels * g->V;
+  // records tag into the sketched levels 0..store_first-1 (every level unless the exact tier is adaptive)
+  const uint32_t sketched = g->store_first;
   PairTag t;
-  t.V = g->V; t.num_levels = g->num_levels; t.L = g->num_subgraphs; t.fixed_level = fixed_level;
+  t.V = g->V; t.num_levels = sketched; t.L = g->num_subgraphs; t.fixed_level = fixed_level;
   t.cs_mix = gs_seed_mix(g->seed);
-  const bool tagged = g->num_levels > 1 && fixed_level < 0;
+  const bool tagged = sketched > 1 && fixed_level < 0;
+  const bool no_sketch = fixed_level < 0 && sketched == 0;  // every edge is kept exactly
   for (uint64_t done = 0; done < n;) {
     const uint64_t m = std::min<uint64_t>(n - done, g->max_batch_edges);
     const uint2* p = reinterpret_cast<const uint2*>(d_pairs) + done;
+    if (no_sketch) {
+      GS_TRY(gs_store_ingest(g, reinterpret_cast<const uint32_t*>(p), m, s));
+      GS_TRY(gs_store_maintain(g, s));
+      g->records_total += m;
+      done += m;
+      continue;
+    }
     const uint64_t bound = tagged ? std::max<uint64_t>(g->part_cap, 4 * m) : 2 * m;
     GS_TRY(gs_ensure_ingest_scratch(g, tagged ? std::max<uint64_t>(g->nbr_cap, 4 * m) : 2 * m));
     GS_TRY(ensure_partition_scratch(g, bound));
@@ -1263,6 +1273,7 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
     if (fixed_level < 0) {
       GS_TRY(gs_eager_ingest(g, reinterpret_cast<const uint32_t*>(p), m, s));
       GS_TRY(gs_store_ingest(g, reinterpret_cast<const uint32_t*>(p), m, s));
+      GS_TRY(gs_store_maintain(g, s));
     }
     g->records_total += m;
     done += m;

@@ -94,6 +94,7 @@ struct gs_graph {
                                  // ... [16] ingest error bits carried across a query (32 words)
   uint32_t* h_status = nullptr;  // pinned mirror (32 words)
   uint64_t changes = 0;          // count of calls that changed the sketches
+  uint64_t changes_at_clear = 0; // `changes` right after the last gs_clear (0: none since creation)
 
   // ---- asynchronous query (gs_connected_components_async / gs_query_wait) ----
   bool query_pending = false;
@@ -132,9 +133,19 @@ struct gs_graph {
 
   // ---- exact tier of the deep min-cut levels (gs_store.cu) ----
   GsStoreSlot* d_store = nullptr;     // allocated at the first tagged ingest that needs it
-  uint32_t* d_store_status = nullptr; // [1] error bits [2] slots used [3] scratch counter
+  uint32_t* d_store_status = nullptr; // [0] live edges [1] error bits [2] slots used [3] scratch counter
   uint32_t* h_store = nullptr;        // pinned mirror
   uint32_t store_mask = 0;
+  // sketched levels: records tag into levels 0..min(tag, store_first-1), edges with tag >= store_first
+  // are kept exactly.  store_first starts at store_initial and grows by one per contraction while it
+  // is below num_levels (gs_graph_set_edge_store); without that call it stays num_levels.
+  uint32_t store_first = 1;
+  uint32_t store_initial = 1;
+  bool store_adaptive = false;
+  uint64_t store_budget = 0;          // live edges that trigger a contraction
+  uint64_t store_contractions = 0;
+  uint2* d_store_list = nullptr;      // live edges of the store during a contraction or compaction
+  uint64_t store_list_cap = 0;
 
   // ---- profiling ----
   bool prof_on = false;
@@ -210,6 +221,10 @@ gs_status gs_eager_forest(gs_graph* g, cudaStream_t s);                // the ea
 
 // Exact tier of the deep min-cut levels (gs_store.cu).
 bool gs_store_active(const gs_graph* g);                               // tags can reach past the sketches
+// After an ingest pass: when the store holds store_budget live edges or more and a sketch level is
+// free, its lowest level becomes a sketch level (repeatedly); a store crowded by deleted edges is
+// compacted.  Synchronizes.
+gs_status gs_store_maintain(gs_graph* g, cudaStream_t s);
 gs_status gs_store_ingest(gs_graph* g, const uint32_t* d_pairs, uint64_t n, cudaStream_t s);
 gs_status gs_store_clear(gs_graph* g, cudaStream_t s);
 gs_status gs_store_edges(gs_graph* g, uint32_t min_tag, std::vector<uint32_t>* out, cudaStream_t s);

@@ -232,9 +232,20 @@ class GraphSketch:
               "gs_min_cut")
         return value.value, lvl.value, cut.value, side
 
+    def set_edge_store(self, initial_sketch_levels: int, store_bytes: int = 0) -> None:
+        """gs_graph_set_edge_store: start with `initial_sketch_levels` sketched levels and turn the exact
+        tier's lowest level into a sketch level whenever it holds store_bytes / 16 edges."""
+        check(self._lib.gs_graph_set_edge_store(self._h, initial_sketch_levels, store_bytes), "gs_graph_set_edge_store")
+
+    def sketched_levels(self) -> tuple[int, int]:
+        """(levels sketched now, contractions so far)."""
+        lv, c = C.c_uint32(), C.c_uint64()
+        check(self._lib.gs_graph_sketched_levels(self._h, C.byref(lv), C.byref(c)), "gs_graph_sketched_levels")
+        return lv.value, c.value
+
     def edge_store_edges(self, min_tag: int | None = None) -> np.ndarray:
-        """Present edges of the exact tier with subgraph tag >= min_tag (default: num_levels)."""
-        t = self.num_levels if min_tag is None else min_tag
+        """Present edges of the exact tier with subgraph tag >= min_tag (default: the sketched levels)."""
+        t = self.sketched_levels()[0] if min_tag is None else min_tag
         n = C.c_uint64()
         check(self._lib.gs_edge_store_edges(self._h, t, None, 0, C.byref(n)), "gs_edge_store_edges")
         out = np.empty((max(n.value, 1), 2), np.uint32)

@@ -199,7 +199,7 @@ gs_status gs_disjoint_spanning_forests(gs_graph* g, uint32_t level, uint32_t k, 
 /* Min-cut driver of the reference's tools/min_cut.cu:208-252: for level g = 0,1,... take k
  * disjoint spanning forests, compute the exact minimum cut of their union, and stop at the
  * first level whose cut is < k.  When no sketched level does and tags can pass the sketches
- * (num_subgraphs > num_levels), level g = num_levels answers from the exact tier (see
+ * (num_subgraphs > the sketched levels), the first unsketched level answers from the exact tier (see
  * gs_edge_store_edges) with the exact min cut of all its edges, whatever its value; otherwise
  * the last sketched level answers.
  * value = cut * 2^g.  side (host, length V, may be NULL) receives 1 for vertices on one side. */
@@ -212,12 +212,28 @@ gs_status gs_exact_min_cut(uint32_t num_vertices, const uint32_t* pairs, uint64_
                            uint64_t* value, uint8_t* side);
 
 /* The exact tier of a min-cut graph (EdgeStore, src/edge_store.cpp:60-300; get_edges): edges whose
- * subgraph tag reaches num_levels are also kept exactly on the device, with each toggle flipping
- * their presence; gs_min_cut answers from them when no sketched level certifies a cut below k.
- * Writes the present edges with tag >= min_tag (sorted by edge id, at most `capacity`) and their
- * count to *num_edges.  Empty when num_subgraphs <= num_levels (no tag passes the sketches). */
+ * subgraph tag reaches the sketched levels are also kept exactly on the device, with each toggle
+ * flipping their presence; gs_min_cut answers from them when no sketched level certifies a cut below
+ * k.  Writes the present edges with tag >= min_tag (sorted by edge id, at most `capacity`) and their
+ * count to *num_edges.  Empty when num_subgraphs <= the sketched levels (no tag passes the sketches). */
 gs_status gs_edge_store_edges(gs_graph* g, uint32_t min_tag, uint32_t* edges, uint64_t capacity,
                               uint64_t* num_edges);
+
+/* Makes the exact tier adaptive, as the reference's EdgeStore (src/edge_store.cpp:60-300,
+ * include/mc_gpu_sketch_alg.h:168-230): the graph starts with `initial_sketch_levels` sketched levels
+ * (0 = every edge kept exactly) of its num_levels, and edges whose tag reaches the sketched levels are
+ * kept exactly.  After each ingest pass, when the tier holds at least store_bytes / 16 present edges
+ * (the reference's bound: sketch_bytes / 8 per directed adjacency entry, two per edge; 0 = one sketch
+ * level's bytes) and a level is free, its lowest level becomes a sketch level: the stored edges of
+ * that level and above are XORed into it and only deeper ones stay exact.  gs_min_cut then walks the
+ * levels sketched at query time and answers the next one from the exact tier.  Only on a min-cut graph
+ * (num_subgraphs > 1) with no ingest since creation or gs_clear; gs_clear returns to the initial
+ * levels.  Edges whose tag would be num_subgraphs - 1 or more are tagged num_subgraphs - 1, where the
+ * reference's all-exact start tags them num_subgraphs (src/edge_store.cpp:51): both exceed every level
+ * a graph can sketch. */
+gs_status gs_graph_set_edge_store(gs_graph* g, uint32_t initial_sketch_levels, uint64_t store_bytes);
+/* Levels sketched now (MCGPUSketchAlg::get_num_sketch_graphs) and contractions so far. */
+gs_status gs_graph_sketched_levels(const gs_graph* g, uint32_t* levels, uint64_t* contractions);
 
 /* Copy vertex sketches [first, first+count) of `level` to / from host memory in the
  * contiguous [vertex][num_buckets] Bucket layout of Sketch::serialize

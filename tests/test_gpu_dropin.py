@@ -17,6 +17,7 @@ from stream_file import REFERENCE_FIXTURE, read_stream_file, write_stream_file
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DEMO = os.path.join(ROOT, "gpusketch_b200", "_build", "cc_dropin_demo")
 REF_TOOL = os.path.join(ROOT, "oracle", "_ref", "cuda_process_stream")
+REF_MC_TOOL = os.path.join(ROOT, "oracle", "_ref", "min_cut")
 
 
 @pytest.mark.gpu
@@ -101,3 +102,23 @@ def test_stream_file_ingest_in_ranges(tmp_path, restatement):
         with pytest.raises(gs.GpuSketchError) as e:
             g.ingest_stream_file(trunc)
         assert e.value.status == 7
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(REF_MC_TOOL), reason="the reference tool was not built (no reference tree)")
+@pytest.mark.parametrize("n_block,initial", [(512, 0), (8192, 1)])
+def test_reference_min_cut_tool_runs_unchanged_against_the_dropin(tmp_path, n_block, initial):
+    """tools/min_cut.cu of the reference, compiled without an edit against gpusketch_b200/cpp, on the
+    planted-cut stream written as a binary stream file: at V=1024 its memory estimate allows no sketch
+    graph, so every edge stays exact and the adjacency answers; at V=2^14 (the min-cut workload's size)
+    one sketch level at its reduced_k factor (51 columns) certifies the cut with k=25 forests.  Both
+    print the planted cut of 3."""
+    from gpusketch_b200.workloads import planted_cut_stream
+    recs, _ = planted_cut_stream(n_block)
+    path = str(tmp_path / "planted.data")
+    write_stream_file(path, 2 * n_block, recs)
+    out = subprocess.run([REF_MC_TOOL, path, "4", "2", str(initial)], capture_output=True, text=True, timeout=900,
+                         cwd=str(tmp_path))
+    assert out.returncode == 0, out.stdout[-3000:] + out.stderr[-3000:]
+    final = [l for l in out.stdout.splitlines() if l.startswith("Final mincut value:")]
+    assert len(final) == 1 and float(final[0].split(":")[1]) == 3.0, out.stdout[-3000:]
