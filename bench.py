@@ -55,7 +55,9 @@ def parse_args():
     ap.add_argument("--no-mincut", action="store_true", help="skip the planted-cut min-cut workload")
     ap.add_argument("--batched-streams", type=int, default=256)
     ap.add_argument("--batched-phases", type=int, default=4)
-    ap.add_argument("--served-seconds", type=float, default=1.0, help="length of the served request trace")
+    ap.add_argument("--served-seconds", type=float, default=10.0, help="length of the x1 served request trace")
+    ap.add_argument("--served-loads", default="1,4,16", help="offered-load factors of the served sweep")
+    ap.add_argument("--no-dropin", action="store_true", help="skip the stream-file and C++ drop-in sub-lines")
     return ap.parse_args()
 
 
@@ -67,28 +69,46 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def ncu_issue_per_launch():
-    """warp instructions of one full-size ingest launch from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "k_ingest_rmat17_issue.txt")
+KERNEL_SOURCES = ("gpusketch_b200/csrc/gs_ingest.cu", "gpusketch_b200/csrc/gs_common.cuh")
+
+
+def kernel_source_sha16() -> str:
+    """sha256 (first 16 hex digits) of the sketch-update kernel's sources, as the ncu summaries record
+    it: a committed capture describes the current kernel only when the two agree."""
+    import hashlib
+    h = hashlib.sha256()
+    for rel in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def _profile_field(name: str, key: str):
+    """(value, source sha16 recorded with it) from a committed ncu summary in profiles/."""
+    value = sha = None
     try:
-        for line in open(path):
-            if line.startswith("warp_instructions_per_full_launch:"):
-                return float(line.split(":", 1)[1])
+        for line in open(os.path.join(ROOT, "profiles", name)):
+            if line.startswith(key + ":"):
+                value = float(line.split(":", 1)[1])
+            elif line.startswith("source_sha256_16:"):
+                sha = line.split(":", 1)[1].strip()
     except OSError:
         pass
-    return None
+    return value, sha
+
+
+def ncu_issue_per_launch():
+    """warp instructions of one full-size ingest launch from the committed ncu summary, and whether that
+    capture ran the current kernel sources."""
+    v, sha = _profile_field("k_ingest_rmat17_issue.txt", "warp_instructions_per_full_launch")
+    return v, sha == kernel_source_sha16()
 
 
 def ncu_traffic_per_launch():
-    """dram bytes read+write of one full-size ingest launch from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "k_ingest_rmat17_traffic.txt")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_full_launch:"):
-                return float(line.split(":", 1)[1])
-    except OSError:
-        pass
-    return None
+    """dram bytes read+write of one full-size ingest launch from the committed ncu summary, and whether
+    that capture ran the current kernel sources."""
+    v, sha = _profile_field("k_ingest_rmat17_traffic.txt", "traffic_bytes_per_full_launch")
+    return v, sha == kernel_source_sha16()
 
 
 class ClockSampler:
@@ -302,7 +322,11 @@ def run_batched(args, dev, steps, warmup):
         return out
 
     plain_step()
-    plain_s, plain_res = timed(plain_step, 1)
+    plain_runs = []
+    for _ in range(3):
+        t, plain_res = timed(plain_step, 1)
+        plain_runs.append(t)
+    plain_s = statistics.median(plain_runs)
     for h in handles:
         h.close()
     agree = all(plain_res[p][t] == eng_res[p][t][0] == eager_res[p][t][0] for p in range(P) for t in ids)
@@ -312,45 +336,145 @@ def run_batched(args, dev, steps, warmup):
         "engine_value": total / eng_s, "engine_eager_value": total / eager_s, "plain_value": total / plain_s,
         "unit": UNIT, "speedup_vs_plain": plain_s / eng_s, "engine_ms_per_step": 1e3 * eng_s,
         "engine_eager_ms_per_step": 1e3 * eager_s, "plain_ms_per_step": 1e3 * plain_s,
+        "plain_ms_per_step_runs": [1e3 * t for t in plain_runs],
         "engine_eager_split_ms_per_step": {k: prof[k] / steps for k in ("ingest_ms", "bucket_ms", "query_ms")},
         "cuda_graphs": {"instantiated": built, "launched": launched},
         "tuning": tune, "answers_agree": agree,
-        "timing": "wall clock per step around synchronous calls, device idle on both sides",
+        "timing": "wall clock per step around synchronous calls, device idle on both sides; plain: median of 3 steps",
     }
 
 
-def run_served(args, dev):
-    """64 tenants (V = round(2^U(10,16)), R-MAT records), Poisson arrivals (mean gap 2 ms), update
-    batches of round(2^U(10,20)) records from page-locked host buffers, 10% connectivity queries;
-    replayed in real time by the continuous-batching server and by the plain per-tenant server."""
+def _served_once(tr, dev, with_plain: bool) -> dict:
     import torch
     from gpusketch_b200.engine import tenant_bytes
     from gpusketch_b200.serve import PlainServer, SketchServer
-    from gpusketch_b200.workloads import served_trace
-
-    tr = served_trace(64, args.served_seconds)
     need = sum(tenant_bytes(v) for v, _, _ in tr.tenants)
     srv = SketchServer(tr, need + (256 << 20), device=dev.index)
     host = srv.prepare()
     payloads = [torch.from_numpy(a.astype("int32")).pin_memory() if a is not None else None for a in host]
+    del host
     srv.run(payloads, time_scale=0.05)  # warm-up pass 20x faster than real time; every tenant retires
     st = srv.run(payloads)
     srv.close()
-    plain = PlainServer(tr, device=dev.index)
-    pst = plain.run(payloads)
-    plain.close()
-
     offered = sum(r.n for r in tr.requests if r.kind == "update")
+    out = {"requests": len(tr.requests), "queries": len(st.answers), "offered_updates": offered,
+           "offered_updates_per_s": offered / tr.duration_s, "updates_per_s": st.updates_per_s,
+           "query_latency_ms": st.latency_summary(), "ingest_calls": st.ingest_calls,
+           "query_launches": st.query_launches, "wall_s": st.wall_s, "max_live_tenants": st.max_live_tenants,
+           "sketch_bytes_needed": need}
+    if with_plain:
+        plain = PlainServer(tr, device=dev.index)
+        pst = plain.run(payloads)
+        plain.close()
+        out["plain_query_latency_ms"] = pst.latency_summary()
+        out["plain_updates_per_s"] = pst.updates_per_s
+        out["plain_wall_s"] = pst.wall_s
+    del payloads
+    return out
+
+
+def run_served(args, dev):
+    """64 tenants (V = round(2^U(10,16)), R-MAT records), Poisson arrivals, update batches of
+    round(2^U(10,20)) records from page-locked host buffers, 10% connectivity queries; replayed in real
+    time by the continuous-batching server.  The offered load is swept: at load x f the mean gap is
+    2/f ms and the trace lasts served_seconds/f, so every point offers the same records and about as
+    many queries (about 500 at 10 s).  The plain per-tenant server replays the x1 trace."""
+    from gpusketch_b200.workloads import served_trace
+
+    loads = [float(x) for x in args.served_loads.split(",")]
+    sweep = []
+    for f in loads:
+        tr = served_trace(64, args.served_seconds / f, mean_gap_ms=2.0 / f)
+        point = _served_once(tr, dev, with_plain=(f == 1.0))
+        point["load"] = f
+        point["trace_seconds"] = tr.duration_s
+        sweep.append(point)
+    base = next((p for p in sweep if p["load"] == 1.0), sweep[0])
+    crossing = next((p["load"] for p in sweep if p["query_latency_ms"]["p99"] > 10.0), None)
     return {
-        "workload": "served_64_tenants_rmat", "scope": "one GPU (rank 0)", "tenants": len(tr.tenants), "requests": len(tr.requests),
-        "queries": len(st.answers), "trace_seconds": args.served_seconds, "offered_updates": offered,
-        "query_latency_ms": st.latency_summary(), "updates_per_s": st.updates_per_s,
-        "plain_query_latency_ms": pst.latency_summary(), "plain_updates_per_s": pst.updates_per_s,
-        "ingest_calls": st.ingest_calls, "query_launches": st.query_launches,
-        "plain_ingest_calls": pst.ingest_calls, "wall_s": st.wall_s, "plain_wall_s": pst.wall_s,
-        "max_live_tenants": st.max_live_tenants, "sketch_bytes_needed": need,
+        "workload": "served_64_tenants_rmat", "scope": "one GPU (rank 0)", "tenants": 64,
+        "trace_seconds": args.served_seconds, "requests": base["requests"], "queries": base["queries"],
+        "offered_updates": base["offered_updates"], "query_latency_ms": base["query_latency_ms"],
+        "updates_per_s": base["updates_per_s"], "plain_query_latency_ms": base.get("plain_query_latency_ms"),
+        "plain_updates_per_s": base.get("plain_updates_per_s"), "ingest_calls": base["ingest_calls"],
+        "query_launches": base["query_launches"], "wall_s": base["wall_s"],
+        "max_live_tenants": base["max_live_tenants"], "sketch_bytes_needed": base["sketch_bytes_needed"],
+        "load_sweep": [{k: p[k] for k in ("load", "trace_seconds", "offered_updates_per_s", "updates_per_s",
+                                          "queries", "query_latency_ms", "wall_s")} for p in sweep],
+        "p99_over_10ms_from_load": crossing,
         "latency": "enqueue (trace arrival time) to answer, wall clock",
     }
+
+
+def run_dropin(args, dev):
+    """Stream files and the reference-facing C++ classes, one GPU:
+    * file_ingest: a 2^27-record binary stream file (the reference's format, 1.2 GB, R-MAT V=2^17) read by
+      the library (gs_ingest_stream_file: parallel pread into the page-locked ring, device decode),
+      timed from the call to the end of the device work; the file is in the page cache;
+    * reference_tool: the reference's own tools/cuda_process_stream.cu, compiled unchanged against the
+      drop-in headers, on the same file: its "Updates per second" line (GraphSketchDriver ->
+      CCGPUSketchAlg, insertion time including the final flush);
+    * apply_update_batch: the reference's worker path on the first 2^26 records - per-vertex batches of
+      get_desired_updates_per_batch() destinations (grouped on the host, untimed) handed to
+      CCGPUSketchAlg::apply_update_batch from 8 worker threads, then flush_buffers and
+      connected_components() (timed)."""
+    import tempfile
+    import numpy as np
+    import torch
+    import gpusketch_b200 as gs
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from stream_file import write_stream_file
+
+    out = {"scope": "one GPU (rank 0)"}
+    V = 1 << V_LOG2
+    n = 1 << 27
+    d = torch.empty((n, 2), dtype=torch.int32, device=dev)
+    gs.rmat_stream(V_LOG2, n, STREAM_SEED, out=d)
+    host = d.cpu().numpy().view(np.uint32)
+    del d
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "rmat17_2p27.data")
+        write_stream_file(path, V, host, types=np.zeros(n, np.uint8))
+        small = os.path.join(tmp, "rmat17_2p26.data")
+        write_stream_file(small, V, host[: 1 << 26], types=np.zeros(1 << 26, np.uint8))
+        del host
+        fbytes = os.path.getsize(path)
+        with gs.GraphSketch(V, SKETCH_SEED, device=dev.index) as g:
+            g.ingest_stream_file(path, 0, 1 << 20)        # warm-up: staging ring, scratch
+            g.clear()
+            g.synchronize()
+            rates = []
+            for _ in range(3):
+                g.clear()
+                g.synchronize()
+                t0 = time.perf_counter()
+                got = g.ingest_stream_file(path)
+                g.synchronize()
+                rates.append(got / (time.perf_counter() - t0))
+        r = statistics.median(rates)
+        out["file_ingest"] = {"records": n, "file_bytes": fbytes, "updates_per_s": r, "file_gb_per_s": r * 9 / 1e9,
+                              "runs": rates, "timing": "wall clock, call to end of device work, median of 3"}
+        tool = os.path.join(ROOT, "oracle", "_ref", "cuda_process_stream")
+        if os.path.exists(tool):
+            res = subprocess.run([tool, path, "8", "2"], capture_output=True, text=True, timeout=600, cwd=tmp)
+            line = [l for l in res.stdout.splitlines() if l.startswith("Updates per second:")]
+            cc = [l for l in res.stdout.splitlines() if l.startswith("Connected Components:")]
+            out["reference_tool"] = {"tool": "tools/cuda_process_stream.cu (unchanged) + drop-in headers",
+                                     "rc": res.returncode,
+                                     "updates_per_s": float(line[0].split(":")[1]) if line else None,
+                                     "connected_components": int(cc[0].split(":")[1]) if cc else None}
+        demo = os.path.join(ROOT, "gpusketch_b200", "_build", "cc_dropin_demo")
+        if os.path.exists(demo):
+            res = subprocess.run([demo, small, str(SKETCH_SEED), "-", "1", "batches"], capture_output=True, text=True,
+                                 timeout=900, cwd=tmp)
+            line = [l for l in res.stdout.splitlines() if l.startswith("updates=")]
+            f = dict(kv.split("=") for kv in line[0].split()) if line else {}
+            out["apply_update_batch"] = {"records": 1 << 26, "rc": res.returncode,
+                                         "updates_per_s": float(f["updates_per_sec"]) if f else None,
+                                         "batches": int(f["batches"]) if f else None,
+                                         "seconds": float(f["seconds"]) if f else None,
+                                         "path": "CCGPUSketchAlg::apply_update_batch x 8 threads + flush + CC"}
+    return out
 
 
 def run_mincut(args, dev):
@@ -366,8 +490,13 @@ def run_mincut(args, dev):
     recs, _ = planted_cut_stream(n)
     V = 2 * n
     L = 1 + 2 * int(np.log2(V))
+    # the sketch size the reference's min-cut tool uses: sketches_factor = reduced_k
+    # (tools/min_cut.cu:95-96,156), 51 samples per sketch at V=2^14
+    k_tool = int(np.ceil(np.log2(V) / 0.75 ** 2))
+    reduced_k = (k_tool / np.log2(V)) * 1.5
     d = torch.from_numpy(recs.astype(np.int32)).to(dev)
-    g = gs.GraphSketch(V, 0x5EED0003, num_levels=4, num_subgraphs=L, device=dev.index, max_batch_edges=1 << 25)
+    g = gs.GraphSketch(V, 0x5EED0003, sketches_factor=reduced_k, num_levels=4, num_subgraphs=L, device=dev.index,
+                       max_batch_edges=1 << 25)
     g.ingest_pairs(d)            # warm-up of the same work, then cleared
     g.min_cut(4)
     g.clear()
@@ -380,7 +509,10 @@ def run_mincut(args, dev):
     t2 = time.perf_counter()
     g.close()
     return {"workload": "mincut_planted_v16384", "scope": "one GPU (rank 0)", "records": int(len(recs)),
-            "levels": 4, "k": 4, "num_subgraphs": L, "ingest_updates_per_s": len(recs) / (t1 - t0),
+            "levels": 4, "k": 4, "num_subgraphs": L, "sketches_factor": reduced_k,
+            "sketch_columns": gs.geometry_for(V, reduced_k).num_columns,
+            "sketch_bytes_per_vertex_level": gs.geometry_for(V, reduced_k).bytes_per_vertex,
+            "ingest_updates_per_s": len(recs) / (t1 - t0),
             "ingest_ms": 1e3 * (t1 - t0), "min_cut_ms": 1e3 * (t2 - t1), "value": value, "expected": 3,
             "level": level, "cut_at_level": cut_at,
             "timing": "wall clock around synchronous calls, device idle on both sides"}
@@ -465,20 +597,23 @@ def run_gs(args):
     ingest_ms_avg = prof["ingest_ms"] / launches
     achieved = alg_per_launch / (ingest_ms_avg / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
+    traffic, traffic_current = ncu_traffic_per_launch()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": ncu_traffic_per_launch(), "peak_source": peak_kind,
+                "traffic": traffic, "traffic_source": "committed ncu capture (profiles/k_ingest_rmat17_traffic.txt)",
+                "traffic_capture_matches_source": traffic_current, "peak_source": peak_kind,
                 "kernel": "k_ingest_packed (sketch update)", "alg_bytes_per_launch": alg_per_launch,
                 "avg_launch_ms": ingest_ms_avg, "path_frac": value / world * (alg_step / U) / 1e9 / peak}
     # the sketch update is bound by instruction issue: its measured warp instructions per launch
     # (one-pass ncu count of this workload's launch) against 4 schedulers x SMs x the sampled SM clock
     issue = None
-    inst = ncu_issue_per_launch()
+    inst, inst_current = ncu_issue_per_launch()
     if inst is not None and V == (1 << 17) and phase == (1 << 27) and clocks.get("sm_mhz"):
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         ach = inst / (ingest_ms_avg / 1e3)
         pk = 4.0 * sms * clocks["sm_mhz"] * 1e6
         issue = {"bound": "issue", "achieved": ach, "peak": pk, "unit": "warp_inst/s", "frac": ach / pk,
-                 "inst_per_launch": inst, "kernel": "k_ingest_packed (sketch update)",
+                 "inst_per_launch": inst, "inst_source": "committed ncu capture (profiles/k_ingest_rmat17_issue.txt)",
+                 "inst_capture_matches_source": inst_current, "kernel": "k_ingest_packed (sketch update)",
                  "peak_source": f"4 schedulers x {sms} SMs x median sampled SM clock"}
     split = {"ingest_ms_per_step": prof["ingest_ms"] / args.steps, "bucket_ms_per_step": prof["bucket_ms"] / args.steps,
              "query_ms_per_step": prof["query_ms"] / args.steps}
@@ -525,9 +660,14 @@ def run_gs(args):
     g.close()
     del d_in
     torch.cuda.empty_cache()
-    batched = served = mincut = None
+    batched = served = mincut = dropin = None
     if not args.no_mincut:
         mincut = run_mincut(args, dev)
+    if not args.no_dropin and rank == 0:
+        try:
+            dropin = run_dropin(args, dev)
+        except Exception as exc:  # a sub-line, never required
+            dropin = {"error": str(exc)}
     if not args.no_batched:
         batched = run_batched(args, dev, max(1, args.steps), max(1, args.warmup))
     if not args.no_served:
@@ -548,7 +688,7 @@ def run_gs(args):
         "roofline": roofline, "issue_roofline": issue, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": prof["kernel_launches"],
         "clocks": clocks, "kernel_split": split, "batched": batched, "served": served,
-        "mincut": mincut,
+        "mincut": mincut, "dropin": dropin,
     }
     if os.environ.get("GS_BENCH_TUNE_TABLE"):
         line["tune_table"] = tune_table

@@ -442,6 +442,86 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter(const uint2* __re
   }
 }
 
+// pass 2, placement with one-word records, sorted in shared memory: a block loads its chunk once
+// (kVertChunk / kPartThreads records per thread, held in registers), counts them per vertex, reserves
+// each vertex's run in the output, sorts the chunk by vertex into a shared stage (the record keeps its
+// bucket-local key in its top bits), and writes the stage out with consecutive threads on consecutive
+// addresses of each vertex's run.  The scattered one-record stores of k_vert_scatter cost one L2 sector
+// request per record; these cost one per 32 bytes of a run.
+constexpr int kVertPer = kVertChunk / kPartThreads;   // records per thread per chunk
+static_assert(kVertPer * kPartThreads == kVertChunk, "a chunk is a whole number of records per thread");
+
+size_t vert_scatter_sorted_smem(uint32_t lb) {
+  return (size_t)4 * (1u << lb) * sizeof(uint32_t) + (size_t)kVertChunk * sizeof(uint32_t);
+}
+
+__global__ void __launch_bounds__(kPartThreads) k_vert_scatter_sorted(const uint32_t* __restrict__ part,
+                                                                      const uint32_t* __restrict__ bkt, uint32_t H,
+                                                                      uint32_t lb, uint32_t* __restrict__ cursor,
+                                                                      uint32_t* __restrict__ nbr, uint64_t cap,
+                                                                      uint32_t* __restrict__ status) {
+  extern __shared__ uint32_t sh[];
+  __shared__ uint32_t s_d;
+  const uint32_t nk = 1u << lb;
+  uint32_t* hist = sh;            // [nk] records per vertex of the chunk
+  uint32_t* loff = sh + nk;       // [nk] first stage slot of each vertex
+  uint32_t* base = sh + 2 * nk;   // [nk] first output position of each vertex's run
+  uint32_t* cur = sh + 3 * nk;    // [nk] stage cursors
+  uint32_t* stage = sh + 4 * nk;  // [kVertChunk] records sorted by vertex
+  const uint32_t* off = bkt + H;
+  const uint32_t* choff = bkt + 3 * H + 1;
+  const uint32_t shift = 32u - lb, umask = (1u << shift) - 1u;
+  const uint32_t total = status[5];
+  for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+    if (threadIdx.x == 0) s_d = chunk_bucket(choff, H, c);
+    for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const uint32_t d = s_d;
+    const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
+    const uint32_t r1 = min(off[d + 1], r0 + kVertChunk);
+    uint32_t rec[kVertPer];
+#pragma unroll
+    for (int j = 0; j < kVertPer; j++) {
+      const uint32_t i = r0 + threadIdx.x + j * blockDim.x;
+      rec[j] = i < r1 ? part[i] : 0xffffffffu;
+    }
+#pragma unroll
+    for (int j = 0; j < kVertPer; j++)
+      if (r0 + threadIdx.x + j * blockDim.x < r1) atomicAdd(&hist[rec[j] >> shift], 1u);
+    __syncthreads();
+    // block scan of the counts (thread t owns vertices [t*per, (t+1)*per)) and the global reservations
+    {
+      const uint32_t per = (nk + blockDim.x - 1) / blockDim.x;
+      const uint32_t k0 = min(nk, threadIdx.x * per), k1 = min(nk, k0 + per);
+      uint32_t sum = 0;
+      for (uint32_t k = k0; k < k1; k++) sum += hist[k];
+      uint2 tot;
+      uint32_t run = block_exclusive_scan(make_uint2(sum, 0u), &tot).x;
+      for (uint32_t k = k0; k < k1; k++) {
+        const uint32_t h = hist[k];
+        loff[k] = run;
+        cur[k] = run;
+        base[k] = h ? atomicAdd(&cursor[(d << lb) + k], h) : 0u;
+        run += h;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kVertPer; j++)
+      if (r0 + threadIdx.x + j * blockDim.x < r1) stage[atomicAdd(&cur[rec[j] >> shift], 1u)] = rec[j];
+    __syncthreads();
+    const uint32_t n = r1 - r0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t r = stage[i];
+      const uint32_t k = r >> shift;
+      const uint32_t pos = base[k] + (i - loff[k]);
+      if (pos < cap) nbr[pos] = r & umask;
+      else atomicOr(&status[0], (uint32_t)GS_DEV_ERR_CAPACITY);
+    }
+    __syncthreads();
+  }
+}
+
 // Directed per-vertex batches: batch b adds sizes[b] records to vertex level*V + srcs[b].
 __global__ void k_count_batches(const uint32_t* __restrict__ srcs, const uint64_t* __restrict__ sizes,
                                 uint32_t nb, uint32_t V, uint32_t level, uint32_t* __restrict__ cnt,
@@ -1121,6 +1201,22 @@ gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& 
   return GS_OK;
 }
 
+gs_status launch_vert_scatter_sorted(const uint2* part, const uint32_t* bkt, uint32_t H, uint32_t lb, uint32_t* cursor,
+                                     uint32_t* nbr, uint64_t cap, uint32_t* status, int grid, cudaStream_t s) {
+  const size_t smem = vert_scatter_sorted_smem(lb);
+  static thread_local size_t smem_set[64] = {};
+  int dev = 0;
+  GS_CUDA_TRY(cudaGetDevice(&dev));
+  if (smem_set[dev & 63] < smem) {
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_vert_scatter_sorted, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    smem_set[dev & 63] = smem;
+  }
+  k_vert_scatter_sorted<<<grid, kPartThreads, smem, s>>>(reinterpret_cast<const uint32_t*>(part), bkt, H, lb, cursor,
+                                                          nbr, cap, status);
+  GS_CUDA_TRY(cudaGetLastError());
+  return GS_OK;
+}
+
 }  // namespace
 
 gs_status gs_ensure_ingest_scratch(gs_graph* g, uint64_t records) {
@@ -1256,8 +1352,8 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
       if (compact) {
         k_vert_count<true><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status);
         GS_TRY(scan_counts(g, nv, s));
-        k_vert_scatter<true><<<grid2, kPartThreads, vs_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr,
-                                                                  g->nbr_cap, g->d_status);
+        GS_TRY(launch_vert_scatter_sorted(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status,
+                                          grid2, s));
       } else {
         k_vert_count<false><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status);
         GS_TRY(scan_counts(g, nv, s));

@@ -70,6 +70,7 @@ class Request:
 class ServedTrace:
     tenants: list[tuple[int, int, int]]  # (V, log2 of the R-MAT space, sketch seed)
     requests: list[Request] = field(default_factory=list)
+    duration_s: float = 0.0              # length of the arrival process
 
     def tenant_records(self, tenant: int, first: int, n: int) -> np.ndarray:
         """Records [first, first+n) of a tenant's stream, on the host (counter-based: any range)."""
@@ -85,7 +86,7 @@ def served_trace(num_tenants: int = 64, duration_s: float = 1.0, mean_gap_ms: fl
     for i in range(num_tenants):
         V = int(round(2.0 ** rng.uniform(10.0, 16.0)))
         tenants.append((V, max(1, math.ceil(math.log2(V))), 0xC0FFEE + 0x100 + i))
-    tr = ServedTrace(tenants)
+    tr = ServedTrace(tenants, duration_s=duration_s)
     cursor = [0] * num_tenants
     t = 0.0
     while True:
