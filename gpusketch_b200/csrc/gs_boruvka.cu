@@ -597,6 +597,9 @@ gs_status gs_boruvka_enqueue(gs_graph* g, uint32_t level, uint32_t round0_col, c
     GS_TRY(gs_boruvka_launch(L, s));
   }
   GS_CUDA_TRY(cudaMemcpyAsync(h_out, g->d_status, 17 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  // the query's error bits are read back with its words: the error word starts clean for the ingest
+  // calls queued after the query (a stale bit would fail the next synchronizing call)
+  GS_CUDA_TRY(cudaMemsetAsync(g->d_status, 0, sizeof(uint32_t), s));
   return GS_OK;
 }
 
