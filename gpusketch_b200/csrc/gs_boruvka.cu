@@ -208,6 +208,8 @@ struct BorArgs {
                                // [12] accumulate work counter
   uint32_t* tstate;            // [T][4]: done, modified this round, rounds, out of samples
   uint64_t wait_ns;            // grid-barrier wait limit
+  uint32_t complement;         // T == 1 with a zero-sum sketch set: see the accumulate phase
+  unsigned long long* largest; // (size << 32) | ~root of the round's largest component (status 18-19)
 };
 
 __device__ __forceinline__ const GsBorTenant& tenant_of(const BorArgs& A, uint32_t t) {
@@ -249,7 +251,10 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
   const uint32_t span = A.V - A.vlo;
 
   for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.parent[v] = v;
-  if (gtid == 0) *nroots_p = 0;
+  if (gtid == 0) {
+    *nroots_p = 0;
+    if (A.complement) *A.largest = 0ull;
+  }
   if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
 
   for (uint32_t round = 0; round < A.max_rounds; round++) {
@@ -278,6 +283,23 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
       }
       if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
 
+      // ---- complement: the round's largest component (ties to the smallest root) ----
+      if (A.complement) {
+        const uint32_t nr = ld_volatile(nroots_p);
+        unsigned long long best = 0ull;
+        for (uint32_t k = gtid; k < nr; k += gthreads) {
+          const uint32_t r = __ldcg(&A.roots[k]);
+          const unsigned long long key = ((unsigned long long)__ldcg(&A.size[r]) << 32) | (0xffffffffu - r);
+          best = key > best ? key : best;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+          best = other > best ? other : best;
+        }
+        if (lane == 0 && best) atomicMax(A.largest, best);
+        if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
+      }
+
       // ---- accumulate column r + the deterministic bucket per component ----
       // Warps take runs of kAccGrab vertices from a shared counter (finished tenants' vertices cost
       // almost nothing, so fixed slices would leave most warps idle at the barrier) and walk each
@@ -286,9 +308,20 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
       // that is flushed with red.global.xor when the component changes.  A vertex whose root is
       // another vertex is in a component of two or more, so only roots read their own size: no load
       // hammers a giant component's root.
+      //
+      // Complement (one graph whose sketch set XORs to zero, because every update reached both
+      // endpoints): the XOR of ALL vertex sketches is zero, so the largest component's merged column
+      // equals the XOR of the columns of every vertex outside it.  Its members are then skipped, and
+      // every other vertex - singletons included - is folded into the largest component's row as well
+      // as its own.  A round reads the vertices outside the largest component instead of all of them.
       {
+        const unsigned long long big =
+            A.complement ? *reinterpret_cast<const volatile unsigned long long*>(A.largest) : 0ull;
+        const uint32_t cbig = (big >> 32) > 1ull ? 0xffffffffu - (uint32_t)big : 0xffffffffu;
         uint32_t cur = 0xffffffffu, w = 0;
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
+        uint64_t ca[3] = {0, 0, 0}, cg[3] = {0, 0, 0};   // the largest component's row (complement)
+        bool any_c = false;
         for (;;) {
           uint32_t g0 = 0;
           if (lane == 0) g0 = atomicAdd(acc_next, kAccGrab);
@@ -298,15 +331,23 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         for (uint32_t start = A.vlo + g0; start < w1; start += kAccRun) {
           const uint32_t n = min(kAccRun, w1 - start);
           uint32_t rt = 0xffffffffu, tt = 0;
+          bool outside = false;   // folded into the largest component's row (complement)
           if (lane < n) {
             const uint32_t v = start + lane;
             tt = A.vtenant ? A.vtenant[v] : 0u;
             if (!s_done[tt]) {
               const uint32_t r = __ldcg(&A.parent[v]);
-              if (r != v || __ldcg(&A.size[v]) > 1u) rt = r;
+              if (cbig != 0xffffffffu) {
+                outside = r != cbig;
+                if (outside && (r != v || __ldcg(&A.size[v]) > 1u)) rt = r;
+              } else if (r != v || __ldcg(&A.size[v]) > 1u) {
+                rt = r;
+              }
             }
           }
-          const uint32_t live = __ballot_sync(0xffffffffu, rt != 0xffffffffu);
+          const uint32_t own = __ballot_sync(0xffffffffu, rt != 0xffffffffu);
+          const uint32_t outm = __ballot_sync(0xffffffffu, outside);
+          const uint32_t live = own | outm;
           for (uint32_t m = live; m;) {
             const uint32_t i = __ffs(m) - 1;
             m &= m - 1;
@@ -320,11 +361,25 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
           for (uint32_t m = live; m;) {
             const uint32_t i = __ffs(m) - 1;
             m &= m - 1;
+            const uint32_t wi = tenant_of(A, __shfl_sync(0xffffffffu, tt, i)).bkt + 1;
+            if ((outm >> i) & 1u) {
+              any_c = true;
+#pragma unroll
+              for (int k = 0; k < 3; k++) {
+                const uint32_t j = lane + 32u * k;
+                if (j < wi) {
+                  const GsBucket b = stage[i * A.W + j];
+                  ca[k] ^= b.alpha;
+                  cg[k] ^= b.gamma;
+                }
+              }
+            }
+            if (!((own >> i) & 1u)) continue;
             const uint32_t root = __shfl_sync(0xffffffffu, rt, i);
             if (root != cur) {
               if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
               cur = root;
-              w = tenant_of(A, __shfl_sync(0xffffffffu, tt, i)).bkt + 1;
+              w = wi;
 #pragma unroll
               for (int k = 0; k < 3; k++) a[k] = gm[k] = 0;
             }
@@ -342,6 +397,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         }
         }
         if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
+        if (any_c) flush_acc(A, cbig, A.t0.bkt + 1, ca, cg);
       }
       if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
     }
@@ -471,6 +527,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
     if (gtid == 0) {
       *nroots_p = 0;
       *acc_next = 0;
+      if (A.complement) *A.largest = 0ull;
     }
     for (uint32_t t = gtid; t < A.T; t += gthreads) {
       volatile uint32_t* ts = A.tstate + 4 * t;
@@ -519,6 +576,9 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
   A.status = L.status;
   A.tstate = L.tstate;
   A.wait_ns = L.wait_ns;
+  A.complement = (L.T == 1 && L.complement) ? 1u : 0u;
+  // status words 18-19 (only a graph's 32-word status array is used with the complement)
+  A.largest = A.complement ? reinterpret_cast<unsigned long long*>(L.status + 18) : nullptr;
   int dev = 0;
   GS_CUDA_TRY(cudaGetDevice(&dev));
   const size_t smem = (size_t)((L.T + 3u) & ~3u) * sizeof(uint32_t) + (size_t)kWarps * kAccRun * L.W * sizeof(GsBucket);
@@ -582,6 +642,7 @@ gs_status gs_boruvka_enqueue(gs_graph* g, uint32_t level, uint32_t round0_col, c
   L.status = g->d_status;
   L.tstate = g->d_status + 8;
   L.wait_ns = g->wait_ns;
+  L.complement = g->sketches_symmetric ? 1u : 0u;
 
   // the kernel expects all-zero accumulator rows and leaves them so when it runs to the end
   if (g->acc_dirty) GS_CUDA_TRY(cudaMemsetAsync(g->d_acc, 0, (size_t)V * (bkt + 1) * sizeof(GsBucket), s));

@@ -204,6 +204,7 @@ gs_status gs_clear(gs_graph* g) {
   std::fill(g->sample_cursor.begin(), g->sample_cursor.end(), 0u);
   g->store_first = g->store_initial;
   g->changes_at_clear = g->changes;
+  g->sketches_symmetric = true;
   GS_TRY(gs_store_clear(g, g->stream));
   return gs_eager_reset_empty(g, g->stream);
 }
@@ -396,6 +397,7 @@ gs_status gs_ingest_vertex_batches(gs_graph* g, uint32_t level, const uint32_t* 
   cudaStream_t s = pick_stream(g, stream);
   g->labels_valid = false;
   g->changes++;
+  g->sketches_symmetric = false;  // one-sided updates: the XOR of all vertex sketches is no longer zero
   if (on_device) {
     GS_TRY(gs_ingest_device_batches(g, level, srcs, starts, sizes, nbat, dsts, s));
     return order_after(g, s);
@@ -696,6 +698,7 @@ gs_status gs_upload_sketches(gs_graph* g, uint32_t level, uint32_t first, uint32
   const size_t nb = g->geom.num_buckets;
   GS_CUDA_TRY(cudaMemcpy(g->d_sk + ((size_t)level * g->V + first) * nb, host_in, (size_t)count * nb * sizeof(GsBucket),
                          cudaMemcpyHostToDevice));
+  g->sketches_symmetric = false;  // arbitrary bytes: nothing is known about their XOR
   g->labels_valid = false;
   g->changes++;
   return gs_eager_invalidate(g, g->stream);

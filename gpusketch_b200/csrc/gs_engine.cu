@@ -483,7 +483,7 @@ gs_status gs_engine_create(const gs_engine_config* cfg, gs_engine** out) {
   GS_CUDA_TRY(cudaGetLastError());
   GS_CUDA_TRY(cudaMalloc(&e->d_tstate, (size_t)T1 * 4 * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMallocHost(&e->h_tstate, (size_t)T1 * 4 * sizeof(uint32_t)));
-  GS_CUDA_TRY(cudaMalloc(&e->d_qstatus, 16 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMalloc(&e->d_qstatus, 32 * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMallocHost(&e->h_qstatus, 16 * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMalloc(&e->d_q, (size_t)2 * T1 * sizeof(uint32_t)));
   GS_CUDA_TRY(cudaMallocHost(&e->h_q, (size_t)2 * T1 * sizeof(uint32_t)));

@@ -120,6 +120,10 @@ struct gs_graph {
   bool labels_valid = false;     // d_parent holds the partition of the last query
   uint32_t labels_level = 0;
   uint64_t wait_ns = kGsDefaultWaitNs;  // limit of the Boruvka kernel's grid-barrier waits
+  // Every update so far reached both endpoints' sketches (edge records, forests XORed out and back),
+  // so on every level the XOR of all vertex sketches is zero.  One-sided vertex batches and uploaded
+  // sketches clear it; gs_clear sets it again.
+  bool sketches_symmetric = true;
 
   // ---- eager DSU (gs_eager.cu): connectivity kept current by the ingest path ----
   bool eager_on = false;
@@ -255,6 +259,10 @@ struct GsBorLaunch {
   uint32_t* status = nullptr;            // 8 words: [0] errors [4] forest edges [5] running tenants [6,7] barrier
   uint32_t* tstate = nullptr;            // [T][4]: done, modified, rounds, out of samples
   uint64_t wait_ns = kGsDefaultWaitNs;   // grid-barrier wait limit
+  // T == 1 only, and only when the XOR of all vertex sketches of the level is zero (every update
+  // reached both endpoints): the largest component's merged column is taken as the XOR of the vertices
+  // outside it, so the accumulate phase never reads the largest component's own members.
+  uint32_t complement = 0;
 };
 
 // All Boruvka rounds of every tenant in one cooperative launch (queued on s, no host sync).

@@ -498,3 +498,29 @@ def test_async_ingest_and_query_overlap_phases(restatement, pinned):
     with pytest.raises(gs.GpuSketchError):
         with gs.GraphSketch(V, seed) as g2:
             g2.query_wait()                                      # nothing queued
+
+
+@pytest.mark.parametrize("V,n", [(5000, 60000), (1 << 17, 1 << 22)])
+def test_complement_accumulation_equals_direct(restatement, V, n):
+    """A sketch set that XORs to zero lets Boruvka take the largest component's merged column as the
+    XOR of every vertex outside it.  The same sketches re-uploaded (after which the library no longer
+    assumes that) run the direct accumulation: partitions, round counts and forests are equal, and
+    equal the oracle's; both forests span it."""
+    import torch
+    d = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+    gs.rmat_stream(int(np.log2(V)) if V & (V - 1) == 0 else 13, n, 0x5EED3600, out=d)
+    pairs = d.cpu().numpy().view(np.uint32) % np.uint32(V)
+    with gs.GraphSketch(V, 0x5EED3601) as g:
+        g.ingest_pairs(pairs)
+        a_labels, a_ncc, a_rounds = g.connected_components()
+        a_forest = g.spanning_forest()
+        g.upload(g.download())                                   # same bytes, symmetry no longer assumed
+        b_labels, b_ncc, b_rounds = g.connected_components()
+        b_forest = g.spanning_forest()
+    assert (a_ncc, a_rounds) == (b_ncc, b_rounds) and np.array_equal(a_labels, b_labels)
+    # which edge of a cycle of sampled edges loses its union depends on timing: compare what forests are
+    assert len(a_forest) == len(b_forest) == V - a_ncc
+    for f in (a_forest, b_forest):
+        assert np.array_equal(restatement.cc_of_edges(V, f)[1], a_labels)
+    n_exact, exact = restatement.exact_cc(V, pairs)
+    assert a_ncc == n_exact and np.array_equal(a_labels, exact)
