@@ -208,9 +208,15 @@ struct BorArgs {
                                // [12] accumulate work counter
   uint32_t* tstate;            // [T][4]: done, modified this round, rounds, out of samples
   uint64_t wait_ns;            // grid-barrier wait limit
-  uint32_t complement;         // T == 1 with a zero-sum sketch set: see the accumulate phase
-  unsigned long long* largest; // (size << 32) | ~root of the round's largest component (status 18-19)
+  uint32_t complement;         // every tenant's sketch set XORs to zero: see the accumulate phase
+  unsigned long long* largest; // [T] (size << 32) | ~root of each tenant's largest component this round
 };
+
+// root of tenant t's largest component this round, or ~0 when it has no component of two or more
+__device__ __forceinline__ uint32_t largest_root(const BorArgs& A, uint32_t t) {
+  const unsigned long long k = *reinterpret_cast<const volatile unsigned long long*>(A.largest + t);
+  return (k >> 32) > 1ull ? 0xffffffffu - (uint32_t)k : 0xffffffffu;
+}
 
 __device__ __forceinline__ const GsBorTenant& tenant_of(const BorArgs& A, uint32_t t) {
   return A.tenants ? A.tenants[t] : A.t0;
@@ -251,10 +257,9 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
   const uint32_t span = A.V - A.vlo;
 
   for (uint32_t v = A.vlo + gtid; v < A.V; v += gthreads) A.parent[v] = v;
-  if (gtid == 0) {
-    *nroots_p = 0;
-    if (A.complement) *A.largest = 0ull;
-  }
+  if (gtid == 0) *nroots_p = 0;
+  if (A.complement)
+    for (uint32_t t = gtid; t < A.T; t += gthreads) A.largest[t] = 0ull;
   if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
 
   for (uint32_t round = 0; round < A.max_rounds; round++) {
@@ -283,20 +288,28 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
       }
       if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
 
-      // ---- complement: the round's largest component (ties to the smallest root) ----
+      // ---- complement: each tenant's largest component this round (ties to the smallest root) ----
       if (A.complement) {
         const uint32_t nr = ld_volatile(nroots_p);
-        unsigned long long best = 0ull;
-        for (uint32_t k = gtid; k < nr; k += gthreads) {
-          const uint32_t r = __ldcg(&A.roots[k]);
-          const unsigned long long key = ((unsigned long long)__ldcg(&A.size[r]) << 32) | (0xffffffffu - r);
-          best = key > best ? key : best;
+        if (A.T == 1) {
+          unsigned long long best = 0ull;
+          for (uint32_t k = gtid; k < nr; k += gthreads) {
+            const uint32_t r = __ldcg(&A.roots[k]);
+            const unsigned long long key = ((unsigned long long)__ldcg(&A.size[r]) << 32) | (0xffffffffu - r);
+            best = key > best ? key : best;
+          }
+          for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+            best = other > best ? other : best;
+          }
+          if (lane == 0 && best) atomicMax(A.largest, best);
+        } else {
+          for (uint32_t k = gtid; k < nr; k += gthreads) {
+            const uint32_t r = __ldcg(&A.roots[k]);
+            const uint32_t sz = __ldcg(&A.size[r]);
+            if (sz > 1u) atomicMax(A.largest + A.vtenant[r], ((unsigned long long)sz << 32) | (0xffffffffu - r));
+          }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-          const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
-          best = other > best ? other : best;
-        }
-        if (lane == 0 && best) atomicMax(A.largest, best);
         if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
       }
 
@@ -309,19 +322,17 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
       // another vertex is in a component of two or more, so only roots read their own size: no load
       // hammers a giant component's root.
       //
-      // Complement (one graph whose sketch set XORs to zero, because every update reached both
-      // endpoints): the XOR of ALL vertex sketches is zero, so the largest component's merged column
-      // equals the XOR of the columns of every vertex outside it.  Its members are then skipped, and
-      // every other vertex - singletons included - is folded into the largest component's row as well
-      // as its own.  A round reads the vertices outside the largest component instead of all of them.
+      // Complement (sketch sets that XOR to zero, because every update reached both endpoints): the
+      // XOR of ALL of a graph's vertex sketches is zero, so its largest component's merged column
+      // equals the XOR of the columns of every vertex of the graph outside it.  The largest
+      // component's members are then skipped, and every other vertex - singletons included - is
+      // folded into its graph's largest-component row as well as its own.  A round reads the vertices
+      // outside the largest components instead of all of them.
       {
-        const unsigned long long big =
-            A.complement ? *reinterpret_cast<const volatile unsigned long long*>(A.largest) : 0ull;
-        const uint32_t cbig = (big >> 32) > 1ull ? 0xffffffffu - (uint32_t)big : 0xffffffffu;
         uint32_t cur = 0xffffffffu, w = 0;
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
-        uint64_t ca[3] = {0, 0, 0}, cg[3] = {0, 0, 0};   // the largest component's row (complement)
-        bool any_c = false;
+        uint32_t ccur = 0xffffffffu, cw = 0;              // the largest-component row being folded
+        uint64_t ca[3] = {0, 0, 0}, cg[3] = {0, 0, 0};
         for (;;) {
           uint32_t g0 = 0;
           if (lane == 0) g0 = atomicAdd(acc_next, kAccGrab);
@@ -330,15 +341,16 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
           const uint32_t w1 = A.vlo + min(span, g0 + kAccGrab);
         for (uint32_t start = A.vlo + g0; start < w1; start += kAccRun) {
           const uint32_t n = min(kAccRun, w1 - start);
-          uint32_t rt = 0xffffffffu, tt = 0;
-          bool outside = false;   // folded into the largest component's row (complement)
+          uint32_t rt = 0xffffffffu, tt = 0, cb = 0xffffffffu;
+          bool outside = false;   // folded into its graph's largest-component row cb (complement)
           if (lane < n) {
             const uint32_t v = start + lane;
             tt = A.vtenant ? A.vtenant[v] : 0u;
             if (!s_done[tt]) {
               const uint32_t r = __ldcg(&A.parent[v]);
-              if (cbig != 0xffffffffu) {
-                outside = r != cbig;
+              if (A.complement) cb = largest_root(A, tt);
+              if (cb != 0xffffffffu) {
+                outside = r != cb;
                 if (outside && (r != v || __ldcg(&A.size[v]) > 1u)) rt = r;
               } else if (r != v || __ldcg(&A.size[v]) > 1u) {
                 rt = r;
@@ -363,7 +375,14 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
             m &= m - 1;
             const uint32_t wi = tenant_of(A, __shfl_sync(0xffffffffu, tt, i)).bkt + 1;
             if ((outm >> i) & 1u) {
-              any_c = true;
+              const uint32_t ci = __shfl_sync(0xffffffffu, cb, i);
+              if (ci != ccur) {
+                if (ccur != 0xffffffffu) flush_acc(A, ccur, cw, ca, cg);
+                ccur = ci;
+                cw = wi;
+#pragma unroll
+                for (int k = 0; k < 3; k++) ca[k] = cg[k] = 0;
+              }
 #pragma unroll
               for (int k = 0; k < 3; k++) {
                 const uint32_t j = lane + 32u * k;
@@ -397,7 +416,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         }
         }
         if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
-        if (any_c) flush_acc(A, cbig, A.t0.bkt + 1, ca, cg);
+        if (ccur != 0xffffffffu) flush_acc(A, ccur, cw, ca, cg);
       }
       if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
     }
@@ -527,8 +546,9 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
     if (gtid == 0) {
       *nroots_p = 0;
       *acc_next = 0;
-      if (A.complement) *A.largest = 0ull;
     }
+    if (A.complement)
+      for (uint32_t t = gtid; t < A.T; t += gthreads) A.largest[t] = 0ull;
     for (uint32_t t = gtid; t < A.T; t += gthreads) {
       volatile uint32_t* ts = A.tstate + 4 * t;
       if (ts[0]) continue;
@@ -576,9 +596,8 @@ gs_status gs_boruvka_launch(const GsBorLaunch& L, cudaStream_t s) {
   A.status = L.status;
   A.tstate = L.tstate;
   A.wait_ns = L.wait_ns;
-  A.complement = (L.T == 1 && L.complement) ? 1u : 0u;
-  // status words 18-19 (only a graph's 32-word status array is used with the complement)
-  A.largest = A.complement ? reinterpret_cast<unsigned long long*>(L.status + 18) : nullptr;
+  A.complement = (L.complement && L.largest) ? 1u : 0u;
+  A.largest = A.complement ? L.largest : nullptr;
   int dev = 0;
   GS_CUDA_TRY(cudaGetDevice(&dev));
   const size_t smem = (size_t)((L.T + 3u) & ~3u) * sizeof(uint32_t) + (size_t)kWarps * kAccRun * L.W * sizeof(GsBucket);
@@ -643,6 +662,7 @@ gs_status gs_boruvka_enqueue(gs_graph* g, uint32_t level, uint32_t round0_col, c
   L.tstate = g->d_status + 8;
   L.wait_ns = g->wait_ns;
   L.complement = g->sketches_symmetric ? 1u : 0u;
+  L.largest = reinterpret_cast<unsigned long long*>(g->d_status + 18);   // status words 18-19
 
   // the kernel expects all-zero accumulator rows and leaves them so when it runs to the end
   if (g->acc_dirty) GS_CUDA_TRY(cudaMemsetAsync(g->d_acc, 0, (size_t)V * (bkt + 1) * sizeof(GsBucket), s));

@@ -157,6 +157,7 @@ struct gs_engine {
   GsBorTenant* d_bor = nullptr;  // [max_tenants + 1]
   uint32_t* d_vtenant = nullptr; // [max_vertices]
   uint32_t* d_tstate = nullptr;  // [(max_tenants + 1) * 4] Boruvka per-tenant state
+  unsigned long long* d_largest = nullptr;  // [max_tenants + 1] largest component of each tenant per round
   uint32_t* h_tstate = nullptr;  // pinned mirror
   uint32_t* d_qstatus = nullptr; // [16] Boruvka status words
   uint32_t* h_qstatus = nullptr; // pinned [16]
@@ -185,7 +186,7 @@ namespace {
 void free_engine(gs_engine* e) {
   if (!e) return;
   if (e->g) gs_free_graph(e->g);
-  cudaFree(e->d_ing); cudaFree(e->d_bor); cudaFree(e->d_vtenant); cudaFree(e->d_tstate);
+  cudaFree(e->d_ing); cudaFree(e->d_bor); cudaFree(e->d_vtenant); cudaFree(e->d_tstate); cudaFree(e->d_largest);
   cudaFree(e->d_qstatus); cudaFree(e->d_q); cudaFree(e->d_ncc);
   for (auto& tb : e->tabs) {
     cudaFree(tb.d_off); cudaFree(tb.d_ten);
@@ -341,6 +342,9 @@ gs_status enqueue_query(gs_engine* e, const QueryPlan& qp, const uint32_t* tenan
   L.forest_cap = e->max_vertices;
   L.status = e->d_qstatus;
   L.tstate = e->d_tstate;
+  // tenants only take edge records, which reach both endpoints: every tenant's sketches XOR to zero
+  L.complement = 1;
+  L.largest = e->d_largest;
   {
     GsProfScope ps(g, GS_PROF_QUERY, s, 2);
     GS_TRY(gs_boruvka_launch(L, s));
@@ -476,6 +480,7 @@ gs_status gs_engine_create(const gs_engine_config* cfg, gs_engine** out) {
 
   GS_CUDA_TRY(cudaMalloc(&e->d_ing, (size_t)T1 * sizeof(GsIngTenant)));
   GS_CUDA_TRY(cudaMalloc(&e->d_bor, (size_t)T1 * sizeof(GsBorTenant)));
+  GS_CUDA_TRY(cudaMalloc(&e->d_largest, (size_t)T1 * sizeof(unsigned long long)));
   GS_CUDA_TRY(cudaMemsetAsync(e->d_ing, 0, (size_t)T1 * sizeof(GsIngTenant), g->stream));
   GS_CUDA_TRY(cudaMemsetAsync(e->d_bor, 0, (size_t)T1 * sizeof(GsBorTenant), g->stream));
   GS_CUDA_TRY(cudaMalloc(&e->d_vtenant, V * sizeof(uint32_t)));

@@ -259,10 +259,12 @@ struct GsBorLaunch {
   uint32_t* status = nullptr;            // 8 words: [0] errors [4] forest edges [5] running tenants [6,7] barrier
   uint32_t* tstate = nullptr;            // [T][4]: done, modified, rounds, out of samples
   uint64_t wait_ns = kGsDefaultWaitNs;   // grid-barrier wait limit
-  // T == 1 only, and only when the XOR of all vertex sketches of the level is zero (every update
-  // reached both endpoints): the largest component's merged column is taken as the XOR of the vertices
-  // outside it, so the accumulate phase never reads the largest component's own members.
+  // Only when every graph's vertex sketches XOR to zero (every update reached both endpoints): each
+  // graph's largest component's merged column is taken as the XOR of the graph's vertices outside it,
+  // so the accumulate phase never reads the largest components' own members.  `largest` is device
+  // scratch of T 64-bit words.
   uint32_t complement = 0;
+  unsigned long long* largest = nullptr;
 };
 
 // All Boruvka rounds of every tenant in one cooperative launch (queued on s, no host sync).
