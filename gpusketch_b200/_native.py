@@ -71,6 +71,7 @@ SIGNATURES = {
     "gs_ingest_pairs": (C.c_int, [_P, _P, C.c_uint64, C.c_int, _P]),
     "gs_ingest_edges": (C.c_int, [_P, _P, _P, C.c_uint64, C.c_int, _P]),
     "gs_ingest_pairs_async": (C.c_int, [_P, _P, C.c_uint64, C.c_int, _P]),
+    "gs_prepare_host_input": (C.c_int, [_P, C.c_uint64]),
     "gs_ingest_stream_file": (C.c_int, [_P, C.c_char_p, C.c_uint64, C.c_uint64, _U64P]),
     "gs_connected_components_async": (C.c_int, [_P, C.c_uint32]),
     "gs_query_wait": (C.c_int, [_P, _P, _U32P, _U32P]),

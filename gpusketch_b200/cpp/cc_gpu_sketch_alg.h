@@ -36,12 +36,14 @@ class CCGPUSketchAlg {
   // The reference's constructor (include/cc_gpu_sketch_alg.h:36, called by tools/cuda_process_stream.cu:126):
   // the sketch seed comes from the SketchParams; the geometry is derived from num_nodes and
   // config.sketches_factor, which gives the sizes the tools compute into the SketchParams.  num_updates
-  // only sized the reference's host buffers; num_threads worker threads may call apply_update_batch.
+  // sizes the host staging; num_threads worker threads may call apply_update_batch.
   CCGPUSketchAlg(node_id_t num_nodes, size_t num_updates, int num_threads, SketchParams sketch_params,
                  CCAlgConfiguration config = CCAlgConfiguration())
       : CCGPUSketchAlg(num_nodes, sketch_params.seed, config) {
-    (void)num_updates;
     num_host_threads = num_threads > 0 ? num_threads : 1;
+    // the stream's records arrive from the host: set up the page-locked staging now, as the
+    // reference sets up its CudaStream buffers here
+    gs_throw_if(gs_prepare_host_input(g, num_updates), "gs_prepare_host_input");
     gs_geometry geo{};
     gs_graph_geometry(g, &geo);
     if ((sketch_params.num_buckets && sketch_params.num_buckets != geo.num_buckets) ||
@@ -80,21 +82,38 @@ class CCGPUSketchAlg {
   void set_eager_dsu(bool on) { gs_throw_if(gs_set_eager_dsu(g, on ? 1 : 0), "gs_set_eager_dsu"); }
   void print_configuration() { std::cout << config << std::endl; }
 
+  // Each worker (thr_id, one thread each as the driver contract has it) fills a buffer of its own, as
+  // the reference gives every worker its own CudaStream (include/cc_gpu_sketch_alg.h:63-67); a full
+  // buffer is shipped under the handle's lock while the other workers keep filling theirs.
   void apply_update_batch(int thr_id, node_id_t src_vertex, const std::vector<node_id_t>& dst_vertices) {
-    (void)thr_id;
-    std::lock_guard<std::mutex> lk(mtx);
     if (update_locked) throw UpdateLockedException();
-    srcs.push_back(src_vertex);
-    starts.push_back(dsts.size());
-    sizes.push_back(dst_vertices.size());
-    dsts.insert(dsts.end(), dst_vertices.begin(), dst_vertices.end());
-    if (dsts.size() >= flush_at) ship_locked();
+    WorkerBuffer& b = worker(thr_id);
+    Batches full;
+    {
+      std::lock_guard<std::mutex> wl(b.mtx);
+      b.q.srcs.push_back(src_vertex);
+      b.q.starts.push_back(b.q.dsts.size());
+      b.q.sizes.push_back(dst_vertices.size());
+      b.q.dsts.insert(b.q.dsts.end(), dst_vertices.begin(), dst_vertices.end());
+      if (b.q.dsts.size() < flush_at) return;
+      std::swap(full, b.q);
+    }
+    // the worker's lock is released before the handle's: flush_buffers takes them in the other order
+    std::lock_guard<std::mutex> lk(mtx);
+    ship(full);
   }
 
   // CCGPUSketchAlg::flush_buffers (src/cc_gpu_sketch_alg.cpp:21-31)
   void flush_buffers() {
     std::lock_guard<std::mutex> lk(mtx);
-    ship_locked();
+    for (auto& b : workers) {
+      Batches q;
+      {
+        std::lock_guard<std::mutex> wl(b.mtx);
+        std::swap(q, b.q);
+      }
+      ship(q);
+    }
     gs_throw_if(gs_synchronize(g), "gs_synchronize");
   }
 
@@ -194,15 +213,25 @@ class CCGPUSketchAlg {
     return out;
   }
 
-  void ship_locked() {
-    if (srcs.empty()) return;
-    gs_throw_if(gs_ingest_vertex_batches(g, 0, srcs.data(), starts.data(), sizes.data(), (uint32_t)srcs.size(),
-                                         dsts.data(), dsts.size(), 0, nullptr),
+  struct Batches {
+    std::vector<uint32_t> srcs;
+    std::vector<uint64_t> starts, sizes;
+    std::vector<uint32_t> dsts;
+  };
+  struct WorkerBuffer {
+    std::mutex mtx;
+    Batches q;
+  };
+  static constexpr int kWorkers = 256;  // thr_id is taken modulo this
+
+  WorkerBuffer& worker(int thr_id) { return workers[(unsigned)thr_id % kWorkers]; }
+
+  // ships batches through the C ABI; the caller holds mtx (the handle is not thread-safe)
+  void ship(const Batches& b) {
+    if (b.srcs.empty()) return;
+    gs_throw_if(gs_ingest_vertex_batches(g, 0, b.srcs.data(), b.starts.data(), b.sizes.data(),
+                                         (uint32_t)b.srcs.size(), b.dsts.data(), b.dsts.size(), 0, nullptr),
                 "gs_ingest_vertex_batches");
-    srcs.clear();
-    starts.clear();
-    sizes.clear();
-    dsts.clear();
   }
 
   node_id_t num_vertices;
@@ -213,9 +242,7 @@ class CCGPUSketchAlg {
   bool update_locked = false;
   size_t flush_at = 1;
   int num_host_threads = 1;
-  std::vector<uint32_t> srcs;
-  std::vector<uint64_t> starts, sizes;
-  std::vector<uint32_t> dsts;
+  std::vector<WorkerBuffer> workers = std::vector<WorkerBuffer>(kWorkers);
 };
 
 // The CPU algorithm's name maps to the same device implementation.

@@ -234,6 +234,41 @@ __device__ __forceinline__ void flush_acc(const BorArgs& A, uint32_t cur, uint32
   }
 }
 
+// The accumulators a warp still holds at the end of the accumulate phase, flushed once per block:
+// warps of a block that hold the same component's row (every warp holds the largest component's)
+// combine them in shared memory, so one warp per block and component issues the global XORs instead
+// of every warp - the atomics on that row serialize in L2.  Called by every thread of the block.
+__device__ void block_flush(const BorArgs& A, uint32_t root, uint32_t w, const uint64_t* a, const uint64_t* gm,
+                            uint32_t* s_root, GsBucket* stage0) {
+  const uint32_t lane = lane_id(), wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  GsBucket* row = stage0 + (size_t)wib * kAccRun * A.W;
+  if (lane == 0) s_root[wib] = root;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const uint32_t j = lane + 32u * k;
+    if (j < w) row[j] = GsBucket{a[k], gm[k]};
+  }
+  __syncthreads();
+  if (root != 0xffffffffu) {
+    bool leader = true;
+    for (uint32_t o = 0; o < wib; o++) leader = leader && s_root[o] != root;
+    if (leader) {
+      uint64_t x[3] = {a[0], a[1], a[2]}, y[3] = {gm[0], gm[1], gm[2]};
+      for (uint32_t o = wib + 1; o < nw; o++) {
+        if (s_root[o] != root) continue;
+        const GsBucket* other = stage0 + (size_t)o * kAccRun * A.W;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const uint32_t j = lane + 32u * k;
+          if (j < w) { x[k] ^= other[j].alpha; y[k] ^= other[j].gamma; }
+        }
+      }
+      flush_acc(A, root, w, x, y);
+    }
+  }
+  __syncthreads();
+}
+
 // done flags of the tenants, copied from tstate into shared memory once per round
 __device__ __forceinline__ void snapshot_done(const BorArgs& A, uint32_t* s_done) {
   for (uint32_t t = threadIdx.x; t < A.T; t += blockDim.x) s_done[t] = ld_volatile(&A.tstate[4 * t]);
@@ -244,6 +279,7 @@ __device__ __forceinline__ void snapshot_done(const BorArgs& A, uint32_t* s_done
 // area of kAccRun x W buckets per warp.
 __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
   extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ uint32_t s_root[kWarps];
   uint32_t* s_done = smem;
   GsBucket* stage = reinterpret_cast<GsBucket*>(smem + ((A.T + 3u) & ~3u)) + (threadIdx.x >> 5) * kAccRun * A.W;
   uint32_t* err = A.status;
@@ -415,8 +451,10 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
           __syncwarp();
         }
         }
-        if (cur != 0xffffffffu) flush_acc(A, cur, w, a, gm);
-        if (ccur != 0xffffffffu) flush_acc(A, ccur, cw, ca, cg);
+        // the warps' last rows: combined per block (the largest component's row, or with the direct
+        // accumulation the giant component's, is held by nearly every warp)
+        block_flush(A, cur, w, a, gm, s_root, stage - (threadIdx.x >> 5) * kAccRun * A.W);
+        block_flush(A, ccur, cw, ca, cg, s_root, stage - (threadIdx.x >> 5) * kAccRun * A.W);
       }
       if (!grid_sync(bcount, bgen, err, A.wait_ns)) return;
     }

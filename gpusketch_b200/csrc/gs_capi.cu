@@ -91,21 +91,43 @@ __global__ void k_interleave(const uint32_t* __restrict__ a, const uint32_t* __r
     out[i] = make_uint2(a[i], b[i]);
 }
 
-uint64_t staging_pairs(const gs_graph* g) { return std::min<uint64_t>(g->max_batch_edges, 1ull << 24); }
+// Host input moves through two staging slots of at most 2^25 pairs (256 MB each side): a slice's
+// copy overlaps the ingest of the previous slice, and larger slices carry the sketch update's fixed
+// per-launch cost (every touched vertex's rows merged once per launch) less often.
+uint64_t staging_limit(const gs_graph* g) { return std::min<uint64_t>(g->max_batch_edges, 1ull << 25); }
 
 }  // namespace
 
-gs_status gs_ensure_pair_staging(gs_graph* g) {
-  if (g->d_pairs) return GS_OK;
-  const uint64_t cap = staging_pairs(g);
-  GS_CUDA_TRY(cudaMalloc(&g->d_pairs, 2 * cap * 2 * sizeof(uint32_t)));
-  GS_CUDA_TRY(cudaMallocHost(&g->h_pin, 2 * cap * 2 * sizeof(uint32_t)));
-  GS_CUDA_TRY(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
-  for (int i = 0; i < 2; i++) {
-    GS_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_copy[i], cudaEventDisableTiming));
-    GS_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_done[i], cudaEventDisableTiming));
+gs_status gs_ensure_pair_staging(gs_graph* g, uint64_t want) {
+  // the ring is sized for the largest host slice asked for so far (at least 2^20 pairs, a power of
+  // two, at most the limit); small graphs fed small batches keep a small ring
+  uint64_t target = 1ull << 20;
+  while (target < want && target < staging_limit(g)) target <<= 1;
+  target = std::min(target, staging_limit(g));
+  if (g->d_pairs && g->pairs_cap >= target) return GS_OK;
+  if (g->d_pairs) {
+    // growing: every copy into and every reader of the old slots must be done
+    GS_CUDA_TRY(cudaStreamSynchronize(g->copy_stream));
+    for (int i = 0; i < 2; i++) GS_CUDA_TRY(cudaEventSynchronize(g->ev_done[i]));
+    GS_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    cudaFree(g->d_pairs);
+    cudaFreeHost(g->h_pin);
+    cudaFree(g->d_file_pairs);
+    g->d_pairs = nullptr;
+    g->h_pin = nullptr;
+    g->d_file_pairs = nullptr;
+    g->pairs_cap = 0;
   }
-  g->pairs_cap = cap;
+  GS_CUDA_TRY(cudaMalloc(&g->d_pairs, 2 * target * 2 * sizeof(uint32_t)));
+  GS_CUDA_TRY(cudaMallocHost(&g->h_pin, 2 * target * 2 * sizeof(uint32_t)));
+  if (!g->copy_stream) {
+    GS_CUDA_TRY(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; i++) {
+      GS_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_copy[i], cudaEventDisableTiming));
+      GS_CUDA_TRY(cudaEventCreateWithFlags(&g->ev_done[i], cudaEventDisableTiming));
+    }
+  }
+  g->pairs_cap = target;
   return GS_OK;
 }
 
@@ -234,7 +256,7 @@ namespace {
 // stays in use until the handle's work is done, and every wait on a slot's earlier slice happens on
 // the device, so copies of this call can run ahead of queries queued before it.
 gs_status ingest_host_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, cudaStream_t s, bool wait_copies) {
-  GS_TRY(gs_ensure_pair_staging(g));
+  GS_TRY(gs_ensure_pair_staging(g, n));
   cudaPointerAttributes attr{};
   const bool pinned = cudaPointerGetAttributes(&attr, pairs) == cudaSuccess && attr.type == cudaMemoryTypeHost;
   cudaGetLastError();
@@ -277,7 +299,9 @@ constexpr uint64_t al16(uint64_t x) { return (x + 15) & ~15ull; }
 // the device half and ingested while the next chunk is gathered.
 gs_status ingest_host_batches(gs_graph* g, uint32_t level, const uint32_t* srcs, const uint64_t* starts,
                               const uint64_t* sizes, uint32_t nbat, const uint32_t* dsts, cudaStream_t s) {
-  GS_TRY(gs_ensure_pair_staging(g));
+  uint64_t ndst = 0;
+  for (uint32_t b = 0; b < nbat; b++) ndst += sizes[b];
+  GS_TRY(gs_ensure_pair_staging(g, ndst / 2 + 3 * (uint64_t)nbat));
   const uint64_t slot_bytes = g->pairs_cap * 2 * sizeof(uint32_t);
   // a slot: batch headers (srcs u32, starts u64, sizes u64) in its first quarter, destinations after
   const uint64_t hb = std::max<uint64_t>(1, (slot_bytes / 4) / 24);
@@ -314,7 +338,7 @@ gs_status ingest_host_batches(gs_graph* g, uint32_t level, const uint32_t* srcs,
     GS_TRY(gs_ingest_device_batches(g, level, reinterpret_cast<const uint32_t*>(d),
                                     reinterpret_cast<const uint64_t*>(d + off_starts),
                                     reinterpret_cast<const uint64_t*>(d + off_sizes), (uint32_t)nb,
-                                    reinterpret_cast<const uint32_t*>(d + off_dsts), s));
+                                    reinterpret_cast<const uint32_t*>(d + off_dsts), s, std::max<uint64_t>(nd, 1)));
     GS_CUDA_TRY(cudaEventRecord(g->ev_done[slot], s));
   }
   return order_after(g, s);
@@ -323,6 +347,17 @@ gs_status ingest_host_batches(gs_graph* g, uint32_t level, const uint32_t* srcs,
 }  // namespace
 
 extern "C" {
+
+gs_status gs_prepare_host_input(gs_graph* g, uint64_t records) {
+  if (!g) { gs_set_error("null handle"); return GS_ERR_BAD_ARG; }
+  GS_GUARD(g);
+  GS_TRY(gs_ensure_pair_staging(g, records));
+  if (!g->d_file_pairs) {
+    const uint64_t per = g->pairs_cap * 2 * sizeof(uint32_t) / 9;  // stream-file records per slice
+    GS_CUDA_TRY(cudaMalloc(&g->d_file_pairs, per * sizeof(uint2)));
+  }
+  return GS_OK;
+}
 
 gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int on_device, void* stream) {
   if (!g || (n && !pairs)) { gs_set_error("gs_ingest_pairs: null argument"); return GS_ERR_BAD_ARG; }
@@ -366,7 +401,7 @@ gs_status gs_ingest_edges(gs_graph* g, const uint32_t* src, const uint32_t* dst,
   cudaStream_t s = pick_stream(g, stream);
   g->labels_valid = false;
   g->changes++;
-  GS_TRY(gs_ensure_pair_staging(g));
+  GS_TRY(gs_ensure_pair_staging(g, n));
   const uint64_t cap = g->pairs_cap;
   for (uint64_t done = 0, k = 0; done < n; k++) {
     const uint64_t m = std::min(cap, n - done);

@@ -78,7 +78,7 @@ extern "C" gs_status gs_ingest_stream_file(gs_graph* g, const char* path, uint64
   cudaStream_t s = g->stream;
   g->labels_valid = false;
   g->changes++;
-  GS_TRY(gs_ensure_pair_staging(g));
+  GS_TRY(gs_ensure_pair_staging(g, ((last - first) * kRecordBytes + 7) / 8));
   const uint64_t slot_bytes = g->pairs_cap * 2 * sizeof(uint32_t);
   const uint64_t per = slot_bytes / kRecordBytes;  // records per slice
   if (!g->d_file_pairs) GS_CUDA_TRY(cudaMalloc(&g->d_file_pairs, per * sizeof(uint2)));

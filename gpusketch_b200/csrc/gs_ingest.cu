@@ -1379,12 +1379,12 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
 
 gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* d_srcs,
                                    const uint64_t* d_starts, const uint64_t* d_sizes, uint32_t nbat,
-                                   const uint32_t* d_dsts, cudaStream_t s) {
+                                   const uint32_t* d_dsts, cudaStream_t s, uint64_t max_records) {
   if (nbat == 0) return GS_OK;
   // directed one-sided updates: the eager DSU cannot follow them
   GS_TRY(gs_eager_invalidate(g, s));
   const uint32_t nv = g->num_levels * g->V;
-  GS_TRY(gs_ensure_ingest_scratch(g, 1));
+  GS_TRY(gs_ensure_ingest_scratch(g, std::max<uint64_t>(max_records, 1)));
   GS_CUDA_TRY(cudaMemsetAsync(g->d_cnt, 0, (size_t)(nv + 1) * sizeof(uint32_t), s));
   {
     GsProfScope ps(g, GS_PROF_BUCKET, s, 4);
@@ -1392,10 +1392,15 @@ gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* 
     GS_CUDA_TRY(cudaGetLastError());
     GS_TRY(scan_counts(g, nv, s));
   }
-  GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  GS_CUDA_TRY(cudaStreamSynchronize(s));
-  const uint64_t recs = g->h_status[1];
-  if (recs > g->nbr_cap) GS_TRY(gs_ensure_ingest_scratch(g, recs));
+  // the record count sizes the neighbour scratch: a caller that knows a bound (the host path: the
+  // sum of the batch sizes) spares the read-back and its wait
+  uint64_t recs = max_records;
+  if (!max_records) {
+    GS_CUDA_TRY(cudaMemcpyAsync(g->h_status, g->d_status, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GS_CUDA_TRY(cudaStreamSynchronize(s));
+    recs = g->h_status[1];
+    if (recs > g->nbr_cap) GS_TRY(gs_ensure_ingest_scratch(g, recs));
+  }
   {
     GsProfScope ps(g, GS_PROF_BUCKET, s, 1);
     k_scatter_batches<<<grid_for(g, (uint64_t)nbat * 32, 256), 256, 0, s>>>(

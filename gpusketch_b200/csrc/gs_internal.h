@@ -192,7 +192,9 @@ struct GsProfScope {
 
 // Partial-support helpers implemented in the .cu files.
 gs_status gs_ensure_ingest_scratch(gs_graph* g, uint64_t records);
-gs_status gs_ensure_pair_staging(gs_graph* g);
+// The page-locked staging ring (two slots) for host slices of up to `want` pairs, grown as needed up to
+// min(max_batch_edges, 2^25); UINT64_MAX sizes it at that limit.
+gs_status gs_ensure_pair_staging(gs_graph* g, uint64_t want = ~0ull);
 // Sizes the single-level ingest scratch for batches of `edges` records, so that a later ingest of
 // at most that many records allocates nothing (required while a stream is being captured).
 gs_status gs_reserve_ingest(gs_graph* g, uint64_t edges);
@@ -204,7 +206,8 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
 // Directed per-vertex batches (already on the device).
 gs_status gs_ingest_device_batches(gs_graph* g, uint32_t level, const uint32_t* d_srcs,
                                    const uint64_t* d_starts, const uint64_t* d_sizes,
-                                   uint32_t nb, const uint32_t* d_dsts, cudaStream_t s);
+                                   uint32_t nb, const uint32_t* d_dsts, cudaStream_t s,
+                                   uint64_t max_records = 0);  // 0: read the record count back
 // Device Boruvka on one level; forest edges stay in g->d_forest.
 gs_status gs_boruvka(gs_graph* g, uint32_t level, uint32_t round0_col, cudaStream_t s);
 // The same in two halves: the launch and the read-back of status words [0, 17) into pinned h_out

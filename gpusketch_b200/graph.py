@@ -144,6 +144,10 @@ class GraphSketch:
         check(self._lib.gs_ingest_pairs(self._h, p, n, int(dev), _device_stream(stream, dev)), "gs_ingest_pairs")
         del keep
 
+    def prepare_host_input(self, records: int) -> None:
+        """gs_prepare_host_input: allocate the page-locked staging ring for host slices of `records` now."""
+        check(self._lib.gs_prepare_host_input(self._h, records), "gs_prepare_host_input")
+
     def ingest_pairs_async(self, pairs, stream=None) -> None:
         """gs_ingest_pairs_async: queue the copies and the ingest without waiting.  A page-locked host
         buffer (a pinned CPU tensor) stays in use until the handle's queued work is done: keep it alive

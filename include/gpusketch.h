@@ -121,6 +121,13 @@ uint64_t gs_desired_updates_per_batch(const gs_graph* g);
 gs_status gs_ingest_pairs(gs_graph* g, const uint32_t* pairs, uint64_t n, int pairs_on_device,
                           void* cuda_stream);
 
+/* Allocates now what host input needs - the page-locked staging ring for slices of up to `records`
+ * records (at most min(max_batch_edges, 2^25)) and the stream-file decode buffer - instead of at the
+ * first host ingest; page-locking hundreds of megabytes takes tens of milliseconds.  Library extension
+ * (the reference's CCGPUSketchAlg constructor sets up its CudaStream buffers the same way,
+ * include/cc_gpu_sketch_alg.h:36-95). */
+gs_status gs_prepare_host_input(gs_graph* g, uint64_t records);
+
 /* gs_ingest_pairs without waiting for host input to be copied: the call queues the copies and the
  * ingest and returns.  For page-locked host memory it returns at once and the buffer stays in use until
  * the handle's queued work is done (gs_synchronize, gs_query_wait, or any synchronous query): the caller

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import gpusketch_b200 as gs
+from stream_file import REFERENCE_FIXTURE, read_stream_file
 
 pytestmark = pytest.mark.gpu
 
@@ -33,7 +34,11 @@ def case_pairs(name, golden_dir):
         return gs.er_stream(256, 0.01, 11, 0.5, 0.2)
     if name == "er4096":
         return gs.er_stream(4096, 0.002, 13, 0.1, 0.5)
-    return gs.rmat_stream(12, 40000, 0x5EED0002)
+    if name == "multiples_file_1024":
+        return read_stream_file(REFERENCE_FIXTURE)[2]
+    if name == "rmat_v2p12":
+        return gs.rmat_stream(12, 40000, 0x5EED0002)
+    raise KeyError(name)
 
 
 @pytest.fixture(scope="module")

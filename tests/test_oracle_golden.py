@@ -66,8 +66,10 @@ def test_sketch_digests_match_reference(restatement, golden_dir):
             pairs = gs.er_stream(4096, 0.002, 13, 0.1, 0.5)
         elif case["name"] == "multiples_file_1024":
             pairs = read_stream_file(REFERENCE_FIXTURE)[2]
-        else:
+        elif case["name"] == "rmat_v2p12":
             pairs = gs.rmat_stream(12, 40000, 0x5EED0002)
+        else:
+            raise KeyError(case["name"])
         assert hashlib.sha256(np.ascontiguousarray(pairs, np.uint32).tobytes()).hexdigest() == case["pairs_sha256"]
         sk = restatement.new_sketches(V)
         restatement.ingest(sk, V, seed, pairs)
