@@ -440,7 +440,8 @@ def run_dropin(args, dev):
         del host
         fbytes = os.path.getsize(path)
         with gs.GraphSketch(V, SKETCH_SEED, device=dev.index) as g:
-            g.ingest_stream_file(path, 0, 1 << 20)        # warm-up: staging ring, scratch
+            g.prepare_host_input(n)                      # the page-locked ring for full-size slices
+            g.ingest_stream_file(path, 0, 1 << 20)        # warm-up: scratch, decode buffer
             g.clear()
             g.synchronize()
             rates = []
