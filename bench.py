@@ -56,7 +56,7 @@ def parse_args():
     ap.add_argument("--batched-streams", type=int, default=256)
     ap.add_argument("--batched-phases", type=int, default=4)
     ap.add_argument("--served-seconds", type=float, default=10.0, help="length of the x1 served request trace")
-    ap.add_argument("--served-loads", default="1,4,16", help="offered-load factors of the served sweep")
+    ap.add_argument("--served-loads", default="1,4,16,64", help="offered-load factors of the served sweep")
     ap.add_argument("--no-dropin", action="store_true", help="skip the stream-file and C++ drop-in sub-lines")
     return ap.parse_args()
 
