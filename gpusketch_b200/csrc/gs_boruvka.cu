@@ -369,12 +369,16 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
         uint32_t ccur = 0xffffffffu, cw = 0;              // the largest-component row being folded
         uint64_t ca[3] = {0, 0, 0}, cg[3] = {0, 0, 0};
+        // with the complement most vertices cost one parent load, so runs are taken eight times larger;
+        // a plain load of the counter first keeps warps that find the work gone off the atomic, which
+        // every warp of the grid would otherwise hit once more at the end of the phase
+        const uint32_t grab = A.complement ? 8u * kAccGrab : kAccGrab;
         for (;;) {
           uint32_t g0 = 0;
-          if (lane == 0) g0 = atomicAdd(acc_next, kAccGrab);
+          if (lane == 0) g0 = ld_volatile(acc_next) >= span ? span : atomicAdd(acc_next, grab);
           g0 = __shfl_sync(0xffffffffu, g0, 0);
           if (g0 >= span) break;
-          const uint32_t w1 = A.vlo + min(span, g0 + kAccGrab);
+          const uint32_t w1 = A.vlo + min(span, g0 + grab);
         for (uint32_t start = A.vlo + g0; start < w1; start += kAccRun) {
           const uint32_t n = min(kAccRun, w1 - start);
           uint32_t rt = 0xffffffffu, tt = 0, cb = 0xffffffffu;
