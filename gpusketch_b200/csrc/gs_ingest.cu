@@ -120,10 +120,14 @@ constexpr int kPartEdges = 4096;      // edges per block in pass 1
 constexpr int kVertChunk = 8192;      // partitioned records per block iteration in pass 2
 constexpr int kMaxBuckets = 4096;
 constexpr int kVertUnroll = 8;        // records a pass-2 thread loads before its shared-memory atomics
+constexpr uint64_t kMaxBlockHistWords = 1ull << 24;  // per-block bucket counts kept between pass-1 kernels (64 MB)
 
+// blockhist (may be null): the block's own histogram is also stored at [blockIdx.x * H], so that the
+// staged placement of the same block need not count its edges again
 __global__ void __launch_bounds__(kPartThreads) k_part_count(const uint2* __restrict__ pairs, uint64_t n, PairTag t,
                                                              uint32_t lb, uint32_t H, uint32_t* __restrict__ tot,
-                                                             uint32_t* __restrict__ status) {
+                                                             uint32_t* __restrict__ status,
+                                                             uint32_t* __restrict__ blockhist) {
   extern __shared__ uint32_t hist[];
   for (uint32_t i = threadIdx.x; i < H; i += blockDim.x) hist[i] = 0;
   __syncthreads();
@@ -150,8 +154,10 @@ __global__ void __launch_bounds__(kPartThreads) k_part_count(const uint2* __rest
     }
   }
   __syncthreads();
-  for (uint32_t d = threadIdx.x; d < H; d += blockDim.x)
+  for (uint32_t d = threadIdx.x; d < H; d += blockDim.x) {
     if (hist[d]) atomicAdd(&tot[d], hist[d]);
+    if (blockhist) blockhist[(size_t)blockIdx.x * H + d] = hist[d];
+  }
 }
 
 // bkt layout: tot[H] | off[H+1] | cur[H] | choff[H+1]; status[1] = records, status[5] = pass-2 chunks
@@ -251,7 +257,8 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint
                                                                       PairTag t, uint32_t lb, uint32_t H,
                                                                       uint32_t* __restrict__ bkt,
                                                                       uint2* __restrict__ part, uint64_t cap,
-                                                                      uint32_t* __restrict__ status) {
+                                                                      uint32_t* __restrict__ status,
+                                                                      const uint32_t* __restrict__ blockhist) {
   extern __shared__ uint32_t sh[];
   uint32_t* hist = sh;            // [H] records per bucket
   uint32_t* loff = sh + H;        // [H] exclusive offsets in the block's sorted order
@@ -261,18 +268,23 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint
   uint2* stage = reinterpret_cast<uint2*>(sh + ((4 * H + 1 + 1) & ~1u));  // [2 * kPartEdges]
   uint32_t* gcur = bkt + 2 * H + 1;
   const uint32_t lvl = t.fixed_level >= 0 ? (uint32_t)t.fixed_level : 0u;
-  for (uint32_t i = threadIdx.x; i < H; i += blockDim.x) hist[i] = 0;
-  __syncthreads();
   const uint64_t e0 = (uint64_t)blockIdx.x * kPartEdges;
   const uint64_t e1 = min(n, e0 + kPartEdges);
-  // out-of-range records were reported by k_part_count; self-loops cancel
-  for (uint64_t b = e0; b < e1; b += blockDim.x) {
-    const uint64_t e = b + threadIdx.x;
-    uint2 p = make_uint2(0, 0);
-    if (e < e1) p = pairs[e];
-    const bool ok = e < e1 && p.x < t.V && p.y < t.V && p.x != p.y;
-    slot_inc(hist, (lvl * t.V + p.x) >> lb, ok);
-    slot_inc(hist, (lvl * t.V + p.y) >> lb, ok);
+  if (blockhist) {
+    // the counts k_part_count took of this same block of edges
+    for (uint32_t i = threadIdx.x; i < H; i += blockDim.x) hist[i] = blockhist[(size_t)blockIdx.x * H + i];
+  } else {
+    for (uint32_t i = threadIdx.x; i < H; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    // out-of-range records were reported by k_part_count; self-loops cancel
+    for (uint64_t b = e0; b < e1; b += blockDim.x) {
+      const uint64_t e = b + threadIdx.x;
+      uint2 p = make_uint2(0, 0);
+      if (e < e1) p = pairs[e];
+      const bool ok = e < e1 && p.x < t.V && p.y < t.V && p.x != p.y;
+      slot_inc(hist, (lvl * t.V + p.x) >> lb, ok);
+      slot_inc(hist, (lvl * t.V + p.y) >> lb, ok);
+    }
   }
   __syncthreads();
   // exclusive scan of the block histogram: thread i owns buckets [i*per, (i+1)*per)
@@ -1186,7 +1198,8 @@ gs_status launch_ingest_s(gs_graph* g, uint32_t nv, bool small, cudaStream_t s) 
 
 template <bool COMPACT>
 gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& t, uint32_t lb, uint32_t H,
-                                     uint32_t* bkt, uint2* part, uint64_t cap, uint32_t* status, cudaStream_t s) {
+                                     uint32_t* bkt, uint2* part, uint64_t cap, uint32_t* status,
+                                     const uint32_t* blockhist, cudaStream_t s) {
   const size_t smem = part_scatter_staged_smem(H);
   static thread_local size_t smem_set[64] = {};
   int dev = 0;
@@ -1196,7 +1209,7 @@ gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& 
     smem_set[dev & 63] = smem;
   }
   const unsigned tiles = (unsigned)((m + kPartEdges - 1) / kPartEdges);
-  k_part_scatter_staged<COMPACT><<<tiles, kPartThreads, smem, s>>>(p, m, t, lb, H, bkt, part, cap, status);
+  k_part_scatter_staged<COMPACT><<<tiles, kPartThreads, smem, s>>>(p, m, t, lb, H, bkt, part, cap, status, blockhist);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
 }
@@ -1261,10 +1274,28 @@ static gs_status ensure_partition_scratch(gs_graph* g, uint64_t records) {
   return GS_OK;
 }
 
+// per-block bucket counts for a pass of m edges (untagged passes; null when the table would be too big)
+static gs_status ensure_blockhist(gs_graph* g, uint64_t m, uint32_t** out) {
+  *out = nullptr;
+  const uint64_t words = (m + kPartEdges - 1) / kPartEdges * (uint64_t)g->part_buckets;
+  if (words == 0 || words > kMaxBlockHistWords) return GS_OK;
+  if (g->blockhist_cap < words) {
+    cudaFree(g->d_blockhist);
+    g->d_blockhist = nullptr;
+    g->blockhist_cap = 0;
+    GS_CUDA_TRY(cudaMalloc(&g->d_blockhist, (size_t)words * sizeof(uint32_t)));
+    g->blockhist_cap = words;
+  }
+  *out = g->d_blockhist;
+  return GS_OK;
+}
+
 gs_status gs_reserve_ingest(gs_graph* g, uint64_t edges) {
   const uint64_t m = std::min<uint64_t>(edges, g->max_batch_edges);
   GS_TRY(gs_ensure_ingest_scratch(g, std::max<uint64_t>(2 * m, 1)));
-  return ensure_partition_scratch(g, std::max<uint64_t>(2 * m, 1));
+  GS_TRY(ensure_partition_scratch(g, std::max<uint64_t>(2 * m, 1)));
+  uint32_t* unused = nullptr;
+  return ensure_blockhist(g, m, &unused);
 }
 
 static gs_status scan_counts(gs_graph* g, uint32_t nv, cudaStream_t s) {
@@ -1320,11 +1351,16 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
     const uint32_t H = g->part_buckets, lb = g->part_lb;
     const unsigned tiles = (unsigned)((m + kPartEdges - 1) / kPartEdges);
     const int grid2 = g->num_sms * 4;
+    // per-block bucket counts handed from the count pass to the staged placement (untagged passes,
+    // while the table stays small: tiles x H words)
+    uint32_t* blockhist = nullptr;
+    if (!tagged) GS_TRY(ensure_blockhist(g, m, &blockhist));
     {
       GsProfScope ps(g, GS_PROF_BUCKET, s, 2);
       GS_CUDA_TRY(cudaMemsetAsync(g->d_bkt, 0, (size_t)H * sizeof(uint32_t), s));
       GS_CUDA_TRY(cudaMemsetAsync(g->d_cnt, 0, (size_t)(nv + 1) * sizeof(uint32_t), s));
-      k_part_count<<<tiles, kPartThreads, H * sizeof(uint32_t), s>>>(p, m, t, lb, H, g->d_bkt, g->d_status);
+      k_part_count<<<tiles, kPartThreads, H * sizeof(uint32_t), s>>>(p, m, t, lb, H, g->d_bkt, g->d_status,
+                                                                     tagged ? nullptr : blockhist);
       k_part_scan<<<1, kScanThreads, 0, s>>>(g->d_bkt, H, g->d_status);
       GS_CUDA_TRY(cudaGetLastError());
     }
@@ -1344,9 +1380,11 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
         k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, m, t, lb, H, g->d_bkt, g->d_part,
                                                                              g->part_cap, g->d_status);
       } else if (compact) {
-        GS_TRY(launch_part_scatter_staged<true>(p, m, t, lb, H, g->d_bkt, g->d_part, g->part_cap, g->d_status, s));
+        GS_TRY(launch_part_scatter_staged<true>(p, m, t, lb, H, g->d_bkt, g->d_part, g->part_cap, g->d_status,
+                                                blockhist, s));
       } else {
-        GS_TRY(launch_part_scatter_staged<false>(p, m, t, lb, H, g->d_bkt, g->d_part, g->part_cap, g->d_status, s));
+        GS_TRY(launch_part_scatter_staged<false>(p, m, t, lb, H, g->d_bkt, g->d_part, g->part_cap, g->d_status,
+                                                 blockhist, s));
       }
       const size_t vc_smem = (1u << lb) * sizeof(uint32_t), vs_smem = 2 * (1u << lb) * sizeof(uint32_t);
       if (compact) {
@@ -1453,7 +1491,7 @@ gs_status gs_ingest_pairs_on_scratch(const GsScratchIngest& x, cudaStream_t s) {
   GS_CUDA_TRY(cudaMemsetAsync(x.bkt, 0, (size_t)H * sizeof(uint32_t), s));
   GS_CUDA_TRY(cudaMemsetAsync(x.cnt, 0, (size_t)(nv + 1) * sizeof(uint32_t), s));
   const uint2* p = reinterpret_cast<const uint2*>(x.pairs);
-  k_part_count<<<tiles, kPartThreads, H * sizeof(uint32_t), s>>>(p, x.n, t, lb, H, x.bkt, x.status);
+  k_part_count<<<tiles, kPartThreads, H * sizeof(uint32_t), s>>>(p, x.n, t, lb, H, x.bkt, x.status, nullptr);
   k_part_scan<<<1, kScanThreads, 0, s>>>(x.bkt, H, x.status);
   k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, x.n, t, lb, H, x.bkt, x.part,
                                                                        x.records_cap, x.status);

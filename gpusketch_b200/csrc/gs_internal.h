@@ -81,6 +81,8 @@ struct gs_graph {
   uint2* d_part = nullptr;     // [part_cap] (key, neighbour) records partitioned by key >> part_lb
   uint64_t part_cap = 0;
   uint32_t* d_bkt = nullptr;   // bucket tables of the partition: tot[H] off[H+1] cur[H] choff[H+1]
+  uint32_t* d_blockhist = nullptr;  // [tiles][H] bucket counts of every pass-1 block
+  uint64_t blockhist_cap = 0;
   uint32_t part_buckets = 0;   // H
   uint32_t part_lb = 9;        // low key bits resolved by the second pass
   uint32_t* d_pairs = nullptr; // staging for host-resident input pairs, 2 x [pairs_cap] u32 pairs
