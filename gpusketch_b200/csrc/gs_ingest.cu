@@ -121,6 +121,7 @@ constexpr int kVertChunk = 8192;      // partitioned records per block iteration
 constexpr int kMaxBuckets = 4096;
 constexpr int kVertUnroll = 8;        // records a pass-2 thread loads before its shared-memory atomics
 constexpr uint64_t kMaxBlockHistWords = 1ull << 24;  // per-block bucket counts kept between pass-1 kernels (64 MB)
+constexpr uint64_t kMaxChunkHistWords = 1ull << 25;  // per-chunk vertex counts kept between pass-2 kernels (128 MB)
 
 // blockhist (may be null): the block's own histogram is also stored at [blockIdx.x * H], so that the
 // staged placement of the same block need not count its edges again
@@ -349,10 +350,13 @@ __device__ __forceinline__ uint32_t chunk_bucket(const uint32_t* choff, uint32_t
 }
 
 // pass 2, counting: records per vertex of each bucket chunk
+// chunkhist (may be null): each chunk's per-vertex counts are also stored at [c << lb], so that the
+// sorted placement of the same chunk need not count it again
 template <bool COMPACT>
 __global__ void __launch_bounds__(kPartThreads) k_vert_count(const uint2* __restrict__ part, const uint32_t* __restrict__ bkt,
                                                              uint32_t H, uint32_t lb, uint32_t* __restrict__ cnt,
-                                                             const uint32_t* __restrict__ status) {
+                                                             const uint32_t* __restrict__ status,
+                                                             uint32_t* __restrict__ chunkhist) {
   extern __shared__ uint32_t hist[];
   __shared__ uint32_t s_d;
   const uint32_t* off = bkt + H;
@@ -378,8 +382,10 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_count(const uint2* __rest
         if (ks[j] != 0xffffffffu) atomicAdd(&hist[ks[j]], 1u);
     }
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < nk; k += blockDim.x)
+    for (uint32_t k = threadIdx.x; k < nk; k += blockDim.x) {
       if (hist[k]) atomicAdd(&cnt[(d << lb) + k], hist[k]);
+      if (chunkhist) chunkhist[((size_t)c << lb) + k] = hist[k];
+    }
     __syncthreads();
   }
 }
@@ -471,7 +477,8 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter_sorted(const uint
                                                                       const uint32_t* __restrict__ bkt, uint32_t H,
                                                                       uint32_t lb, uint32_t* __restrict__ cursor,
                                                                       uint32_t* __restrict__ nbr, uint64_t cap,
-                                                                      uint32_t* __restrict__ status) {
+                                                                      uint32_t* __restrict__ status,
+                                                                      const uint32_t* __restrict__ chunkhist) {
   extern __shared__ uint32_t sh[];
   __shared__ uint32_t s_d;
   const uint32_t nk = 1u << lb;
@@ -486,7 +493,12 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter_sorted(const uint
   const uint32_t total = status[5];
   for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
     if (threadIdx.x == 0) s_d = chunk_bucket(choff, H, c);
-    for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x) hist[i] = 0;
+    if (chunkhist) {
+      // the counts k_vert_count took of this same chunk
+      for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x) hist[i] = chunkhist[((size_t)c << lb) + i];
+    } else {
+      for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x) hist[i] = 0;
+    }
     __syncthreads();
     const uint32_t d = s_d;
     const uint32_t r0 = off[d] + (c - choff[d]) * kVertChunk;
@@ -497,9 +509,11 @@ __global__ void __launch_bounds__(kPartThreads) k_vert_scatter_sorted(const uint
       const uint32_t i = r0 + threadIdx.x + j * blockDim.x;
       rec[j] = i < r1 ? part[i] : 0xffffffffu;
     }
+    if (!chunkhist) {
 #pragma unroll
-    for (int j = 0; j < kVertPer; j++)
-      if (r0 + threadIdx.x + j * blockDim.x < r1) atomicAdd(&hist[rec[j] >> shift], 1u);
+      for (int j = 0; j < kVertPer; j++)
+        if (r0 + threadIdx.x + j * blockDim.x < r1) atomicAdd(&hist[rec[j] >> shift], 1u);
+    }
     __syncthreads();
     // block scan of the counts (thread t owns vertices [t*per, (t+1)*per)) and the global reservations
     {
@@ -1215,7 +1229,8 @@ gs_status launch_part_scatter_staged(const uint2* p, uint64_t m, const PairTag& 
 }
 
 gs_status launch_vert_scatter_sorted(const uint2* part, const uint32_t* bkt, uint32_t H, uint32_t lb, uint32_t* cursor,
-                                     uint32_t* nbr, uint64_t cap, uint32_t* status, int grid, cudaStream_t s) {
+                                     uint32_t* nbr, uint64_t cap, uint32_t* status, const uint32_t* chunkhist, int grid,
+                                     cudaStream_t s) {
   const size_t smem = vert_scatter_sorted_smem(lb);
   static thread_local size_t smem_set[64] = {};
   int dev = 0;
@@ -1225,7 +1240,7 @@ gs_status launch_vert_scatter_sorted(const uint2* part, const uint32_t* bkt, uin
     smem_set[dev & 63] = smem;
   }
   k_vert_scatter_sorted<<<grid, kPartThreads, smem, s>>>(reinterpret_cast<const uint32_t*>(part), bkt, H, lb, cursor,
-                                                          nbr, cap, status);
+                                                          nbr, cap, status, chunkhist);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
 }
@@ -1290,12 +1305,31 @@ static gs_status ensure_blockhist(gs_graph* g, uint64_t m, uint32_t** out) {
   return GS_OK;
 }
 
+// per-chunk vertex counts of pass 2 for `records` one-word records (null when the table would be too big)
+static gs_status ensure_chunkhist(gs_graph* g, uint64_t records, uint32_t** out) {
+  *out = nullptr;
+  // chunks: every bucket's records cut into kVertChunk pieces, at most one partial piece per bucket
+  const uint64_t chunks = records / kVertChunk + g->part_buckets + 1;
+  const uint64_t words = chunks << g->part_lb;
+  if (records == 0 || words > kMaxChunkHistWords) return GS_OK;
+  if (g->chunkhist_cap < words) {
+    cudaFree(g->d_chunkhist);
+    g->d_chunkhist = nullptr;
+    g->chunkhist_cap = 0;
+    GS_CUDA_TRY(cudaMalloc(&g->d_chunkhist, (size_t)words * sizeof(uint32_t)));
+    g->chunkhist_cap = words;
+  }
+  *out = g->d_chunkhist;
+  return GS_OK;
+}
+
 gs_status gs_reserve_ingest(gs_graph* g, uint64_t edges) {
   const uint64_t m = std::min<uint64_t>(edges, g->max_batch_edges);
   GS_TRY(gs_ensure_ingest_scratch(g, std::max<uint64_t>(2 * m, 1)));
   GS_TRY(ensure_partition_scratch(g, std::max<uint64_t>(2 * m, 1)));
   uint32_t* unused = nullptr;
-  return ensure_blockhist(g, m, &unused);
+  GS_TRY(ensure_blockhist(g, m, &unused));
+  return ensure_chunkhist(g, 2 * m, &unused);
 }
 
 static gs_status scan_counts(gs_graph* g, uint32_t nv, cudaStream_t s) {
@@ -1388,12 +1422,16 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
       }
       const size_t vc_smem = (1u << lb) * sizeof(uint32_t), vs_smem = 2 * (1u << lb) * sizeof(uint32_t);
       if (compact) {
-        k_vert_count<true><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status);
+        uint32_t* chunkhist = nullptr;
+        GS_TRY(ensure_chunkhist(g, 2 * m, &chunkhist));
+        k_vert_count<true><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status,
+                                                               chunkhist);
         GS_TRY(scan_counts(g, nv, s));
         GS_TRY(launch_vert_scatter_sorted(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status,
-                                          grid2, s));
+                                          chunkhist, grid2, s));
       } else {
-        k_vert_count<false><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status);
+        k_vert_count<false><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status,
+                                                                nullptr);
         GS_TRY(scan_counts(g, nv, s));
         k_vert_scatter<false><<<grid2, kPartThreads, vs_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr,
                                                                    g->nbr_cap, g->d_status);
@@ -1495,7 +1533,8 @@ gs_status gs_ingest_pairs_on_scratch(const GsScratchIngest& x, cudaStream_t s) {
   k_part_scan<<<1, kScanThreads, 0, s>>>(x.bkt, H, x.status);
   k_part_scatter<<<tiles, kPartThreads, 2 * H * sizeof(uint32_t), s>>>(p, x.n, t, lb, H, x.bkt, x.part,
                                                                        x.records_cap, x.status);
-  k_vert_count<false><<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.status);
+  k_vert_count<false><<<grid2, kPartThreads, (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.status,
+                                                                                nullptr);
   const uint32_t stiles = (nv + kScanTile - 1) / kScanTile;
   k_scan_tiles<<<stiles, kScanThreads, 0, s>>>(x.cnt, nv, x.chunk, x.off, x.choff, x.tile);
   k_scan_top<<<1, kScanThreads, 0, s>>>(x.tile, stiles, x.off, x.choff, nv, x.status);

@@ -83,6 +83,8 @@ struct gs_graph {
   uint32_t* d_bkt = nullptr;   // bucket tables of the partition: tot[H] off[H+1] cur[H] choff[H+1]
   uint32_t* d_blockhist = nullptr;  // [tiles][H] bucket counts of every pass-1 block
   uint64_t blockhist_cap = 0;
+  uint32_t* d_chunkhist = nullptr;  // [chunks][2^lb] vertex counts of every pass-2 chunk
+  uint64_t chunkhist_cap = 0;
   uint32_t part_buckets = 0;   // H
   uint32_t part_lb = 9;        // low key bits resolved by the second pass
   uint32_t* d_pairs = nullptr; // staging for host-resident input pairs, 2 x [pairs_cap] u32 pairs
