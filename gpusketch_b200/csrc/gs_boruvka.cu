@@ -369,10 +369,11 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
         uint32_t ccur = 0xffffffffu, cw = 0;              // the largest-component row being folded
         uint64_t ca[3] = {0, 0, 0}, cg[3] = {0, 0, 0};
-        // with the complement most vertices cost one parent load, so runs are taken eight times larger;
-        // a plain load of the counter first keeps warps that find the work gone off the atomic, which
-        // every warp of the grid would otherwise hit once more at the end of the phase
-        const uint32_t grab = A.complement ? 8u * kAccGrab : kAccGrab;
+        // with the complement most vertices cost one parent load and a run's latency is the cost, so
+        // runs are taken one at a time and spread over every warp; a plain load of the counter first
+        // keeps warps that find the work gone off the atomic, which every warp of the grid would
+        // otherwise hit once more at the end of the phase
+        const uint32_t grab = A.complement ? kAccRun : kAccGrab;
         for (;;) {
           uint32_t g0 = 0;
           if (lane == 0) g0 = ld_volatile(acc_next) >= span ? span : atomicAdd(acc_next, grab);
