@@ -369,15 +369,21 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
         uint32_t ccur = 0xffffffffu, cw = 0;              // the largest-component row being folded
         uint64_t ca[3] = {0, 0, 0}, cg[3] = {0, 0, 0};
-        // with the complement most vertices cost one parent load and a run's latency is the cost, so
-        // runs are taken one at a time and spread over every warp; a plain load of the counter first
-        // keeps warps that find the work gone off the atomic, which every warp of the grid would
-        // otherwise hit once more at the end of the phase
+        // With the complement most vertices cost one parent load, so a run's latency is the cost and
+        // the shared counter's atomics (one L2 address for every grab of the grid) would dominate:
+        // runs are then assigned to warps in a fixed stride.  Otherwise warps take runs from the
+        // counter (a plain load first keeps warps that find the work gone off the atomic).
+        uint32_t stride_next = gwarp * kAccRun;
         const uint32_t grab = A.complement ? kAccRun : kAccGrab;
         for (;;) {
           uint32_t g0 = 0;
-          if (lane == 0) g0 = ld_volatile(acc_next) >= span ? span : atomicAdd(acc_next, grab);
-          g0 = __shfl_sync(0xffffffffu, g0, 0);
+          if (A.complement) {
+            g0 = stride_next;
+            stride_next += gwarps * kAccRun;
+          } else {
+            if (lane == 0) g0 = ld_volatile(acc_next) >= span ? span : atomicAdd(acc_next, grab);
+            g0 = __shfl_sync(0xffffffffu, g0, 0);
+          }
           if (g0 >= span) break;
           const uint32_t w1 = A.vlo + min(span, g0 + grab);
         for (uint32_t start = A.vlo + g0; start < w1; start += kAccRun) {
