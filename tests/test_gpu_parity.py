@@ -529,3 +529,26 @@ def test_complement_accumulation_equals_direct(restatement, V, n):
         assert np.array_equal(restatement.cc_of_edges(V, f)[1], a_labels)
     n_exact, exact = restatement.exact_cc(V, pairs)
     assert a_ncc == n_exact and np.array_equal(a_labels, exact)
+
+
+def test_staging_ring_grows_with_the_host_input(restatement):
+    """The page-locked ring starts small for small host batches and grows (after draining what is queued
+    on it) when a larger batch arrives, also behind queued asynchronous work; gs_prepare_host_input sizes
+    it up front.  The sketches equal the oracle's throughout."""
+    import torch
+    V, seed = 4000, 0x5EED3700
+    rng = np.random.default_rng(37)
+    small = rng.integers(0, V, size=(1000, 2), dtype=np.uint32)
+    big = rng.integers(0, V, size=(3_000_001, 2), dtype=np.uint32)
+    bigger = torch.from_numpy(rng.integers(0, V, size=(5_000_000, 2), dtype=np.uint32).view(np.int32)).pin_memory()
+    with gs.GraphSketch(V, seed) as g:
+        g.ingest_pairs(small)                       # a ring of 2^20 pairs
+        g.ingest_pairs_async(big)                   # pageable: staged, grows the ring to 2^22
+        g.ingest_pairs_async(bigger)                # page-locked and queued: grows again to 2^23
+        g.synchronize()
+        want = np.concatenate([small, big, bigger.numpy().view(np.uint32)])
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, want)
+    with gs.GraphSketch(V, seed) as g:
+        g.prepare_host_input(1 << 23)
+        g.ingest_pairs(big)
+        assert sketch_bytes(g) == oracle_bytes(restatement, V, seed, big)
