@@ -369,15 +369,18 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         uint64_t a[3] = {0, 0, 0}, gm[3] = {0, 0, 0};
         uint32_t ccur = 0xffffffffu, cw = 0;              // the largest-component row being folded
         uint64_t ca[3] = {0, 0, 0}, cg[3] = {0, 0, 0};
-        // With the complement most vertices cost one parent load, so a run's latency is the cost and
-        // the shared counter's atomics (one L2 address for every grab of the grid) would dominate:
-        // runs are then assigned to warps in a fixed stride.  Otherwise warps take runs from the
-        // counter (a plain load first keeps warps that find the work gone off the atomic).
+        // One graph with the complement: most vertices cost one parent load, so runs are assigned to
+        // warps in a fixed stride (measured 0.39 vs 0.52 ms per V=2^17 query against the counter).
+        // Otherwise warps take runs from the shared counter, because finished tenants' vertices cost
+        // almost nothing and fixed slices would leave warps idle (the 256-tenant query: 2.35 ms per
+        // query with the counter, 2.95 with the stride); a plain load first keeps warps that find the
+        // work gone off the atomic.
+        const bool strided = A.complement && A.T == 1;
         uint32_t stride_next = gwarp * kAccRun;
-        const uint32_t grab = A.complement ? kAccRun : kAccGrab;
+        const uint32_t grab = kAccGrab;
         for (;;) {
           uint32_t g0 = 0;
-          if (A.complement) {
+          if (strided) {
             g0 = stride_next;
             stride_next += gwarps * kAccRun;
           } else {
