@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         // work gone off the atomic.
         const bool strided = A.complement && A.T == 1;
         uint32_t stride_next = gwarp * kAccRun;
-        const uint32_t grab = kAccGrab;
+        const uint32_t grab = strided ? kAccRun : kAccGrab;   // vertices per taken piece of work
         for (;;) {
           uint32_t g0 = 0;
           if (strided) {
