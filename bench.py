@@ -441,7 +441,7 @@ def run_dropin(args, dev):
         fbytes = os.path.getsize(path)
         with gs.GraphSketch(V, SKETCH_SEED, device=dev.index) as g:
             g.prepare_host_input(n)                      # the page-locked ring for full-size slices
-            g.ingest_stream_file(path, 0, 1 << 20)        # warm-up: scratch, decode buffer
+            g.ingest_stream_file(path)                   # warm-up: full-size scratch, decode buffer, page cache
             g.clear()
             g.synchronize()
             rates = []

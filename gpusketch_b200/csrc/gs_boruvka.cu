@@ -373,8 +373,8 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
         // warps in a fixed stride (measured 0.39 vs 0.52 ms per V=2^17 query against the counter).
         // Otherwise warps take runs from the shared counter, because finished tenants' vertices cost
         // almost nothing and fixed slices would leave warps idle (the 256-tenant query: 2.35 ms per
-        // query with the counter, 2.95 with the stride); a plain load first keeps warps that find the
-        // work gone off the atomic.
+        // query with the counter, 2.95 with the stride; reading the counter before the atomic, to keep
+        // warps that find the work gone off it, made it 3.05).
         const bool strided = A.complement && A.T == 1;
         uint32_t stride_next = gwarp * kAccRun;
         const uint32_t grab = strided ? kAccRun : kAccGrab;   // vertices per taken piece of work
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(kThreads) k_boruvka(const BorArgs A) {
             g0 = stride_next;
             stride_next += gwarps * kAccRun;
           } else {
-            if (lane == 0) g0 = ld_volatile(acc_next) >= span ? span : atomicAdd(acc_next, grab);
+            if (lane == 0) g0 = atomicAdd(acc_next, grab);
             g0 = __shfl_sync(0xffffffffu, g0, 0);
           }
           if (g0 >= span) break;
