@@ -93,27 +93,27 @@ GS_HD uint64_t gs_concat(uint32_t a, uint32_t b) {
 // (Bucket_Boruvka::get_index_depth, include/bucket.h:54-59).  Computes only the low word of the
 // final xorshift unless it is zero (probability 2^-32).
 __device__ __forceinline__ uint32_t gs_depth_from_mixed(uint64_t x, uint32_t max_depth) {
-  // the shifts are written as multiplies so they issue on the FMA pipe, next to the 64-bit
-  // products, instead of the ALU pipe that carries the XORs: (hi >> 3) = umulhi(hi, 2^29),
-  // (h2:l2) >> 28 = (h2 << 4) | (l2 >> 28) = h2 * 16 ^ umulhi(l2, 16)
+  // (hi >> 3) + 8 is written as umulhi(hi, 2^29) + 8, one multiply-add on the FMA pipe next to the
+  // 64-bit products; the low word of (h2:l2) >> 28 is one funnel shift
   uint64_t h = x * kGsMx2;
   uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
   lo ^= __umulhi(hi, 1u << 29) + 8u;
   h = ((uint64_t)hi << 32) | lo;
   h *= kGsMx2;
   const uint32_t l2 = (uint32_t)h, h2 = (uint32_t)(h >> 32);
-  const uint32_t flo = l2 ^ (h2 * 16u) ^ __umulhi(l2, 16u);
+  const uint32_t flo = l2 ^ __funnelshift_r(l2, h2, 28);
   // ctz of the 64-bit value: the high word only decides when the low word is zero (probability
   // 2^-32), so it is computed in a branch that practically never runs
-  uint32_t d = __clz(__brev(flo));
-  if (__builtin_expect(flo == 0u, 0)) d = 32u + __clz(__brev(h2 ^ (h2 >> 28)));
+  uint32_t d = (uint32_t)__ffs((int)flo) - 1u;
+  if (__builtin_expect(flo == 0u, 0)) d = 32u + __clz(__brev(h2 ^ (h2 >> 28)));  // 64 for a zero hash
   return d < max_depth ? d : max_depth;
 }
 
-// The same depth in two steps, for loops that branch on the depth anyway.  gs_depth_low returns the
-// ctz of the final hash's low word (32 when that word is zero, probability 2^-32), exact whenever it
-// is below 32, and the high product word in *h2; gs_depth_finish completes a low-word depth of 32
-// from the high word and caps it at max_depth.
+// The same depth in two steps, for loops that cap the depth anyway.  gs_depth_low returns the ctz of
+// the final hash's low word, exact whenever that word is non-zero, and ~0u when it is zero
+// (probability 2^-32), with the high product word in *h2; gs_depth_finish completes a low-word depth
+// of 32 or more from the high word and caps it at max_depth.  (__ffs is one instruction fewer than
+// __clz(__brev()), and its ffs(0) - 1 = ~0u is exactly the "look at the high word" signal.)
 __device__ __forceinline__ uint32_t gs_depth_low(uint64_t x, uint32_t* h2_out) {
   uint64_t h = x * kGsMx2;
   uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
@@ -122,11 +122,24 @@ __device__ __forceinline__ uint32_t gs_depth_low(uint64_t x, uint32_t* h2_out) {
   h *= kGsMx2;
   const uint32_t l2 = (uint32_t)h, h2 = (uint32_t)(h >> 32);
   *h2_out = h2;
-  return __clz(__brev(l2 ^ (h2 * 16u) ^ __umulhi(l2, 16u)));
+  return (uint32_t)__ffs((int)(l2 ^ __funnelshift_r(l2, h2, 28))) - 1u;
+}
+
+// min(ctz(final hash's low word), cap) for capbit = 1 << cap, cap < 32: the cap bit is OR-ed in by the
+// same three-input logic op as the xorshift, so the capped depth costs no instruction more than the
+// uncapped one.  A result of cap means "cap or deeper".
+__device__ __forceinline__ uint32_t gs_depth_capped(uint64_t x, uint32_t capbit) {
+  uint64_t h = x * kGsMx2;
+  uint32_t lo = (uint32_t)h, hi = (uint32_t)(h >> 32);
+  lo ^= __umulhi(hi, 1u << 29) + 8u;
+  h = ((uint64_t)hi << 32) | lo;
+  h *= kGsMx2;
+  const uint32_t l2 = (uint32_t)h, h2 = (uint32_t)(h >> 32);
+  return (uint32_t)__ffs((int)((l2 ^ __funnelshift_r(l2, h2, 28)) | capbit)) - 1u;
 }
 
 __device__ __forceinline__ uint32_t gs_depth_finish(uint32_t d_low, uint32_t h2, uint32_t max_depth) {
-  const uint32_t d = d_low < 32u ? d_low : 32u + __clz(__brev(h2 ^ (h2 >> 28)));
+  const uint32_t d = d_low < 32u ? d_low : 32u + __clz(__brev(h2 ^ (h2 >> 28)));  // 64 for a zero hash
   return d < max_depth ? d : max_depth;
 }
 #endif

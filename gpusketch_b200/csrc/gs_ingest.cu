@@ -307,17 +307,26 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint
     if (threadIdx.x == 0) *s_total = tot.x;
   }
   __syncthreads();
-  for (uint64_t b = e0; b < e1; b += blockDim.x) {
-    const uint64_t e = b + threadIdx.x;
-    uint2 p = make_uint2(0, 0);
-    if (e < e1) p = pairs[e];
-    const bool ok = e < e1 && p.x < t.V && p.y < t.V && p.x != p.y;
-    const uint32_t ku = lvl * t.V + p.x, kv = lvl * t.V + p.y;
-    const uint32_t pu = slot_inc(cur, ku >> lb, ok);
-    const uint32_t pv = slot_inc(cur, kv >> lb, ok);
-    if (ok) {
-      stage[pu] = make_uint2(ku, p.y);
-      stage[pv] = make_uint2(kv, p.x);
+  // every load of the block's edges is issued before the first cursor atomic, so the loads overlap
+  for (uint64_t b = e0; b < e1; b += (uint64_t)blockDim.x * kVertUnroll) {
+    uint2 ps[kVertUnroll];
+#pragma unroll
+    for (int j = 0; j < kVertUnroll; j++) {
+      const uint64_t e = b + threadIdx.x + (uint64_t)j * blockDim.x;
+      ps[j] = e < e1 ? pairs[e] : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int j = 0; j < kVertUnroll; j++) {
+      const uint64_t e = b + threadIdx.x + (uint64_t)j * blockDim.x;
+      const uint2 p = ps[j];
+      const bool ok = e < e1 && p.x < t.V && p.y < t.V && p.x != p.y;
+      const uint32_t ku = lvl * t.V + p.x, kv = lvl * t.V + p.y;
+      const uint32_t pu = slot_inc(cur, ku >> lb, ok);
+      const uint32_t pv = slot_inc(cur, kv >> lb, ok);
+      if (ok) {
+        stage[pu] = make_uint2(ku, p.y);
+        stage[pv] = make_uint2(kv, p.x);
+      }
     }
   }
   __syncthreads();
@@ -473,7 +482,9 @@ size_t vert_scatter_sorted_smem(uint32_t lb) {
   return (size_t)4 * (1u << lb) * sizeof(uint32_t) + (size_t)kVertChunk * sizeof(uint32_t);
 }
 
-__global__ void __launch_bounds__(kPartThreads) k_vert_scatter_sorted(const uint32_t* __restrict__ part,
+// three blocks per SM (at most 42 registers a thread): the chunk's records wait in registers while the
+// block scans, and a third resident block keeps loads in flight meanwhile
+__global__ void __launch_bounds__(kPartThreads, 3) k_vert_scatter_sorted(const uint32_t* __restrict__ part,
                                                                       const uint32_t* __restrict__ bkt, uint32_t H,
                                                                       uint32_t lb, uint32_t* __restrict__ cursor,
                                                                       uint32_t* __restrict__ nbr, uint64_t cap,
@@ -668,23 +679,31 @@ struct IngestArgs {
 // ---- packed lane layout (sketches of at most 24 columns) ----
 //
 // With one column per lane, a sketch of C < 32 columns leaves 32 - C lanes idle on every record
-// (8 of 32 at V = 2^17).  The packed layout gives those spare lanes the fourth record of every group
-// of four: a group takes kPackRounds = 3 rounds, in which
-//   * main lane c < C takes column c of records 0, 1, 2 of the group;
-//   * spare lane C + i (i < se = ceil(C / 3) <= 32 - C) takes column i + j se of record 3 in round j
-//     (nothing when that column is >= C).
-// A full batch of 32 staged records takes 24 rounds instead of 32 at C = 24.  Record offset, column
-// constant and row block of every (lane, round) are fixed per geometry and held in registers, so a
-// round costs one hash and one row update like the one-record-per-round loop.  Every lane XORs only
-// into rows of its own, so rounds need no synchronisation: main lane c keeps rows [depth][c] (pitch
-// p1 = C rounded up to 8), spare lane C + i keeps rows [j][depth][lane % 8] (pitch 8; se <= 8, so the
-// spare lanes' residues are distinct).  A lane's entry sits at lane % 8 of its row, so a
-// quarter-warp's accesses stay in distinct bank groups whatever depths its lanes hit.  At the end of
-// a chunk column c gathers its main row and spare slot c / se of lane C + c % se.  Records left over
-// after the groups of four (and every record of a wider sketch) take one round each on the main lanes.
+// (8 of 32 at V = 2^17).  The packed layout covers the C columns of four records with 32 lanes in
+// kPackRounds = 3 steps.  With se = ceil(C / 3) <= 8 and the columns cut into three blocks of se,
+// lane s se + i (slot s < 4, i < se) holds record s of the group for all three steps, and in step j
+//   * a main slot s < 3 takes column i + se ((j + s) mod 3) of its record: in every step the three
+//     main slots cover the three column blocks, so the main lanes touch distinct columns;
+//   * the spare slot s = 3 takes column i + j se of record 3.
+// (nothing when the column is >= C).  A full batch of 32 staged records takes 24 steps instead of 32
+// at C = 24, and a lane loads its record once per group: a 16-byte load costs the same four shared-
+// memory wavefronts whether 8 or 32 lanes share its address, and with the update's read and write of
+// a 16-byte row those wavefronts are the kernel's bound.  Column, column constant and row block of
+// every (lane, step) are fixed per geometry and held in registers.  Column c keeps main rows
+// [depth][c] (pitch p1 = C rounded up to 8) whichever main lane updates it in a step, so the steps are
+// separated by __syncwarp; spare lane 3 se + i keeps its own rows [j][depth][lane % 8] (pitch 8; se <=
+// 8, so the spare lanes' residues are distinct).  A lane's entry sits at its column (main) or lane
+// (spare) mod 8, so a quarter-warp's accesses stay in distinct bank groups whatever depths its lanes
+// hit.  At the end of a chunk column c gathers its main row and the rows of spare lane 3 se + c % se,
+// step c / se.  Records left over after the groups of four (and every record of a wider sketch) take
+// one step each on lanes c < C, lane c taking column c.
 constexpr uint32_t kPackRounds = 3;
 constexpr uint32_t kPackMaxCols = 24;  // ceil(C / 3) <= 32 - C
 constexpr uint32_t kRecWords = 32;
+// rows per lane block: depths 0..kSlabDepth-1 and one discard row, which takes the XOR of every
+// (record, column) that has no row (deeper buckets, spare rounds without a column) so that the hot
+// loop updates a row unconditionally; the discard row is never merged
+constexpr uint32_t kPackRowsAlloc = kSlabDepth + 1;
 // at most 12 warps per block, two blocks per SM: with 8 KB of rows per warp shared memory holds 24
 // warps per SM, and the register cap that two 384-thread blocks leave (85) avoids spills
 constexpr int kPackMaxThreads = 384;
@@ -694,7 +713,7 @@ GS_HD uint32_t pack_p1(uint32_t C) { return (C + 7u) & ~7u; }
 
 // uint4 words per warp: rows of the main lanes and of the spare slots, then the staged records
 GS_HD uint32_t pack_warp_words(uint32_t C) {
-  return (uint32_t)kSlabDepth * (pack_p1(C) + (pack_spare_lanes(C) ? kPackRounds * 8u : 0u)) + kRecWords;
+  return (uint32_t)kPackRowsAlloc * (pack_p1(C) + (pack_spare_lanes(C) ? kPackRounds * 8u : 0u)) + kRecWords;
 }
 
 __device__ __forceinline__ uint32_t chunk_owner(const IngestArgs& A, uint32_t ch, uint32_t lane) {
@@ -927,10 +946,11 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
 
 // Sketch update with the packed lane layout (reg_depth 0, at most 32 columns); chunk lookup, record
 // staging, deep-bucket path and merge as in k_ingest.
-template <bool SMALL, bool TEN>
+template <bool TEN>
 __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const IngestArgs A) {
   extern __shared__ uint4 smem[];
   constexpr uint32_t kRows = kSlabDepth;
+  constexpr uint32_t kRA = kPackRowsAlloc;
   constexpr uint32_t J = kPackRounds;
   const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
   uint4* const wbase = smem + (size_t)wib * A.warp_words;
@@ -939,8 +959,8 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
   uint32_t C = 0, bkt = A.bkt, nb = A.nb, se = 0, p1 = 8;
   const uint32_t V = A.V;
   uint64_t csmix = 0, cmix = 0;
-  // per lane and round of a group: record offset, column constant, row block, column (or >= C: none)
-  uint32_t ro[J], sb[J], col[J], pitch = 0;
+  // per lane: record slot of a group and, per step, column (>= C: none), column constant, row block
+  uint32_t ro = 0, sb[J], col[J], pitch = 0;
   uint64_t cm[J];
   auto set_geometry = [&](uint32_t c_new, const uint64_t* cmt) {
     C = c_new;
@@ -948,15 +968,17 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
     p1 = pack_p1(C);
     csmix = cmt[C];
     cmix = lane < C ? cmt[lane] : 0ull;
-    const bool main = lane < C, spare = !main && lane < C + se;
-    pitch = main ? p1 : 8u;
+    // slot (J + 1: no record of the groups, also every lane of a wider sketch) and index in the slot
+    const uint32_t sl = se ? min(lane / se, J + 1) : J + 1, i = se ? lane % se : 0u;
+    ro = min(sl, J);
+    pitch = sl < J ? p1 : 8u;
 #pragma unroll
     for (uint32_t j = 0; j < J; j++) {
-      ro[j] = main ? j : J;
-      col[j] = main ? lane : (spare ? lane - C + j * se : 0xffffffffu);
-      col[j] = col[j] < C ? col[j] : 0xffffffffu;
-      cm[j] = col[j] < C ? cmt[col[j]] : 0ull;
-      sb[j] = main ? lane : kRows * p1 + (j * kRows) * 8u + (lane & 7u);
+      const uint32_t c = sl < J ? i + se * ((j + sl) % J) : (sl == J ? i + se * j : 0xffffffffu);
+      col[j] = c < C ? c : 0xffffffffu;
+      cm[j] = c < C ? cmt[c] : 0ull;
+      // a main lane without a column uses the discard row of column i
+      sb[j] = sl < J ? (c < C ? c : i) : kRA * p1 + (j * kRA) * 8u + (lane & 7u);
     }
   };
   uint32_t cur_t = 0xffffffffu;
@@ -993,8 +1015,8 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
       skv = A.sk + (size_t)vv * nb;
     }
 
-    const uint32_t zw = kRows * (p1 + (se ? J * 8u : 0u));
-    // every lane main or spare and every spare round with a column (C = 24): no per-round lane test
+    const uint32_t zw = kRA * (p1 + (se ? J * 8u : 0u));
+    // every lane with a column in every step (C = 24): no per-step lane test
     const bool all_live = C + se == 32u && J * se == C;
     for (uint32_t i = lane; i < zw; i += 32) wbase[i] = make_uint4(0, 0, 0, 0);
     uint64_t det_m = 0, det_g = 0;
@@ -1003,22 +1025,47 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
     // 32-bit shared-window addresses: row block bb of this warp at ws + 16 bb, record k at rs + 16 k
     const uint32_t ws = (uint32_t)__cvta_generic_to_shared(wbase);
     const uint32_t rs = (uint32_t)__cvta_generic_to_shared(rec);
-    const uint32_t pitch16 = pitch * 16u;
-    // XOR record q into the lane's column cc at the depth whose low-word part is dl (high product
-    // word h2), rows at row block bb.  Depths below kRows (and below bkt_per_col, which only a SMALL
-    // geometry has under kRows) go to the lane's rows; the rest is the rare HBM path, which also
-    // completes a depth whose low word was zero.
+    const uint32_t pitch16 = pitch * 16u, p116 = p1 * 16u;
+    // cap = min(bkt_per_col, kRows): depths below it are buckets held in the lane's rows, and row cap
+    // is the discard row (depth kRows, or bkt_per_col = no bucket).  Only a geometry with more
+    // buckets per column than rows has buckets deeper than the rows (the rare HBM path).  The cap is
+    // taken per work chunk: the tenants of one engine launch can have either kind of geometry.
+    const uint32_t cap = min(bkt, kRows);
+    const uint32_t capbit = 1u << cap;
+    // XOR record q into the lane's column cc at the depth whose low-word part is dl (gs_depth_low;
+    // high product word h2), rows at row block bb.  Depths below cap go to the lane's rows; a depth of
+    // kRows or more is completed from the high word (also when the low word was zero) and, when it is
+    // below bkt_per_col, goes to HBM; anything else has no bucket.
     auto update = [&](bool live, uint32_t bb, uint32_t cc, uint32_t dl, uint32_t h2, const uint4& q) {
-      const uint32_t d = SMALL ? min(dl, bkt) : dl;
-      if (live && d < (SMALL ? bkt : kRows)) {
-        const uint32_t a = ws + bb * 16u + d * pitch16;
+      if (live && dl < cap) {
+        const uint32_t a = ws + bb * 16u + dl * p116;
         uint4 t;
         asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(t.x), "=r"(t.y), "=r"(t.z), "=r"(t.w) : "r"(a));
         t.x ^= q.x; t.y ^= q.y; t.z ^= q.z; t.w ^= q.w;
         asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" :: "r"(a), "r"(t.x), "r"(t.y), "r"(t.z), "r"(t.w)
                      : "memory");
-      } else if (!SMALL && live) {
+      } else if (live && dl >= kRows) {
         const uint32_t dd = gs_depth_finish(dl, h2, bkt);
+        if (dd < bkt)
+          xor_bucket_global(skv + (size_t)cc * bkt + dd, gs_key_unmix(((uint64_t)q.y << 32) | q.x),
+                            ((uint64_t)q.w << 32) | q.z);
+      }
+    };
+    // The groups' row update, branch-free: the depth comes capped at `cap` (gs_depth_capped), and
+    // rounds without a column use `cap` as well.  A lane whose depth reached kRows (possible only
+    // when bkt_per_col >= kRows) completes it from the full hash on the rare HBM path (`deep`) after
+    // the group.
+    auto rowx = [&](uint32_t bb, uint32_t d, const uint4& q) {
+      const uint32_t a = ws + bb * 16u + d * pitch16;
+      uint4 t;
+      asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(t.x), "=r"(t.y), "=r"(t.z), "=r"(t.w) : "r"(a));
+      t.x ^= q.x; t.y ^= q.y; t.z ^= q.z; t.w ^= q.w;
+      asm volatile("st.shared.v4.u32 [%0], {%1,%2,%3,%4};" :: "r"(a), "r"(t.x), "r"(t.y), "r"(t.z), "r"(t.w)
+                   : "memory");
+    };
+    auto deep = [&](bool live, uint32_t cc, uint32_t dl, uint64_t cmj, const uint4& q) {
+      if (live && dl >= kRows) {
+        const uint32_t dd = gs_depth_from_mixed((((uint64_t)q.y << 32) | q.x) ^ cmj, bkt);
         if (dd < bkt)
           xor_bucket_global(skv + (size_t)cc * bkt + dd, gs_key_unmix(((uint64_t)q.y << 32) | q.x),
                             ((uint64_t)q.w << 32) | q.z);
@@ -1046,32 +1093,51 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
       const uint32_t cnt = min(32u, re - b);
       const uint32_t ng = se ? cnt >> 2 : 0u;
       uint32_t k = 0;
-      // groups of four records; a0..a2: this lane's record of each round
-      uint32_t a0 = rs + ro[0] * 16u, a1 = rs + ro[1] * 16u, a2 = rs + ro[2] * 16u;
+      // groups of four records; ar: this lane's record of the group.  A main column's rows pass to
+      // another lane from one step to the next, hence the __syncwarp after every step.
+      uint32_t ar = rs + ro * 16u;
       uint32_t gi = 0;
       if (all_live) {
-        for (; gi < ng; gi++, k += J + 1, a0 += 16u * (J + 1), a1 += 16u * (J + 1), a2 += 16u * (J + 1)) {
-          const uint4 q0 = lds(a0), q1 = lds(a1), q2 = lds(a2);
-          uint32_t h0, h1, h2;
-          const uint32_t d0 = gs_depth_low(emix(q0) ^ cm[0], &h0);
-          const uint32_t d1 = gs_depth_low(emix(q1) ^ cm[1], &h1);
-          const uint32_t d2 = gs_depth_low(emix(q2) ^ cm[2], &h2);
-          update(true, sb[0], col[0], d0, h0, q0);
-          update(true, sb[1], col[1], d1, h1, q1);
-          update(true, sb[2], col[2], d2, h2, q2);
+#pragma unroll 2
+        for (; gi < ng; gi++, k += J + 1, ar += 16u * (J + 1)) {
+          const uint4 q = lds(ar);
+          const uint64_t e = emix(q);
+          const uint32_t d0 = gs_depth_capped(e ^ cm[0], capbit);
+          const uint32_t d1 = gs_depth_capped(e ^ cm[1], capbit);
+          const uint32_t d2 = gs_depth_capped(e ^ cm[2], capbit);
+          rowx(sb[0], d0, q);
+          __syncwarp();
+          rowx(sb[1], d1, q);
+          __syncwarp();
+          rowx(sb[2], d2, q);
+          __syncwarp();
+          if (max(d0, max(d1, d2)) >= kRows) {
+            deep(true, col[0], d0, cm[0], q);
+            deep(true, col[1], d1, cm[1], q);
+            deep(true, col[2], d2, cm[2], q);
+          }
         }
       }
-      for (; gi < ng; gi++, k += J + 1, a0 += 16u * (J + 1), a1 += 16u * (J + 1), a2 += 16u * (J + 1)) {
-        const uint4 q0 = lds(a0), q1 = lds(a1), q2 = lds(a2);
-        uint32_t h0, h1, h2;
-        const uint32_t d0 = gs_depth_low(emix(q0) ^ cm[0], &h0);
-        const uint32_t d1 = gs_depth_low(emix(q1) ^ cm[1], &h1);
-        const uint32_t d2 = gs_depth_low(emix(q2) ^ cm[2], &h2);
-        update(col[0] < C, sb[0], col[0], d0, h0, q0);
-        update(col[1] < C, sb[1], col[1], d1, h1, q1);
-        update(col[2] < C, sb[2], col[2], d2, h2, q2);
+      for (; gi < ng; gi++, k += J + 1, ar += 16u * (J + 1)) {
+        const uint4 q = lds(ar);
+        const uint64_t e = emix(q);
+        const uint32_t d0 = gs_depth_capped(e ^ cm[0], capbit);
+        const uint32_t d1 = gs_depth_capped(e ^ cm[1], capbit);
+        const uint32_t d2 = gs_depth_capped(e ^ cm[2], capbit);
+        const bool l0 = col[0] < C, l1 = col[1] < C, l2 = col[2] < C;
+        rowx(sb[0], l0 ? d0 : cap, q);
+        __syncwarp();
+        rowx(sb[1], l1 ? d1 : cap, q);
+        __syncwarp();
+        rowx(sb[2], l2 ? d2 : cap, q);
+        __syncwarp();
+        if (max(d0, max(d1, d2)) >= kRows) {
+          deep(l0, col[0], d0, cm[0], q);
+          deep(l1, col[1], d1, cm[1], q);
+          deep(l2, col[2], d2, cm[2], q);
+        }
       }
-      // the rest: one record per round on the main lanes
+      // the rest: one record per step on lanes c < C
       const bool main = lane < C;
       for (; k + 1 < cnt; k += 2) {
         const uint4 q0 = lds(rs + 16u * k), q1 = lds(rs + 16u * (k + 1));
@@ -1096,8 +1162,8 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
       const uint32_t cl = i / kRows, row = i % kRows;
       uint4 t = wbase[row * p1 + cl];
       if (se) {
-        const uint32_t j = cl / se, sl = C + (cl - j * se);
-        const uint4 t2 = wbase[kRows * p1 + (j * kRows + row) * 8u + (sl & 7u)];
+        const uint32_t j = cl / se, sl = J * se + (cl - j * se);
+        const uint4 t2 = wbase[kRA * p1 + (j * kRA + row) * 8u + (sl & 7u)];
         t.x ^= t2.x; t.y ^= t2.y; t.z ^= t2.z; t.w ^= t2.w;
       }
       if (row >= bkt || (t.x | t.y | t.z | t.w) == 0u) continue;
@@ -1165,7 +1231,7 @@ uint32_t packed_warp_words(const gs_graph* g) {
   return w;
 }
 
-template <bool SMALL, bool TEN>
+template <bool TEN>
 gs_status launch_ingest_packed(gs_graph* g, uint32_t nv, cudaStream_t s) {
   IngestArgs A;
   A.off = g->d_off; A.choff = g->d_choff; A.nbr = g->d_nbr; A.sk = g->d_sk; A.colmix = g->d_colmix;
@@ -1181,14 +1247,14 @@ gs_status launch_ingest_packed(gs_graph* g, uint32_t nv, cudaStream_t s) {
   static thread_local Cache cache[64];  // per host thread, device and kernel instantiation
   Cache& cc = cache[g->device < 64 ? g->device : 63];
   if (cc.smem != smem || cc.warps != warps) {
-    GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest_packed<SMALL, TEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GS_CUDA_TRY(cudaFuncSetAttribute(k_ingest_packed<TEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int nb = 0;
-    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest_packed<SMALL, TEN>, warps * 32, smem));
+    GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest_packed<TEN>, warps * 32, smem));
     cc.smem = smem;
     cc.warps = warps;
     cc.blocks = nb > 0 ? nb : 1;
   }
-  k_ingest_packed<SMALL, TEN><<<g->num_sms * cc.blocks, warps * 32, smem, s>>>(A);
+  k_ingest_packed<TEN><<<g->num_sms * cc.blocks, warps * 32, smem, s>>>(A);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
 }
@@ -1197,7 +1263,7 @@ template <int CG, bool SMALL, bool TEN>
 gs_status launch_ingest_r(gs_graph* g, uint32_t nv, cudaStream_t s) {
   switch (g->tune.reg_depth) {
     case 0:
-      if constexpr (CG == 1) return launch_ingest_packed<SMALL, TEN>(g, nv, s);
+      if constexpr (CG == 1) return launch_ingest_packed<TEN>(g, nv, s);
       else return launch_ingest<CG, 0, SMALL, TEN>(g, nv, s);
     case 1: return launch_ingest<CG, 1, SMALL, TEN>(g, nv, s);
     case 3: return launch_ingest<CG, 3, SMALL, TEN>(g, nv, s);
@@ -1428,7 +1494,7 @@ gs_status gs_ingest_device_pairs(gs_graph* g, const uint32_t* d_pairs, uint64_t 
                                                                chunkhist);
         GS_TRY(scan_counts(g, nv, s));
         GS_TRY(launch_vert_scatter_sorted(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_nbr, g->nbr_cap, g->d_status,
-                                          chunkhist, grid2, s));
+                                          chunkhist, g->num_sms * 3, s));
       } else {
         k_vert_count<false><<<grid2, kPartThreads, vc_smem, s>>>(g->d_part, g->d_bkt, H, lb, g->d_cnt, g->d_status,
                                                                 nullptr);

@@ -84,6 +84,38 @@ def test_tenants_match_solo_runs(restatement, device_input):
             assert e.download(t).tobytes() == sk.tobytes()
 
 
+def test_tiny_and_large_tenants_share_a_launch(restatement):
+    """Tenants of at most 23 vertices have fewer buckets per column (bkt_per_col < 10) than the sketch
+    update keeps shared-memory rows, so their deepest buckets are below the rows' end while a large
+    tenant's go past it to HBM.  One launch updates both kinds: every tenant's bytes equal a solo run
+    and the oracle."""
+    rng = np.random.default_rng(21)
+    specs = [
+        (3, 0x5EED2000, 1.0, lambda: gs.er_stream(3, 0.9, 21, 0.1, 0.5)),
+        (12, 0x5EED2001, 1.0, lambda: gs.er_stream(12, 0.5, 22, 0.1, 0.5)),
+        (23, 0x5EED2002, 1.0, lambda: gs.er_stream(23, 0.3, 23, 0.1, 0.5)),
+        (4096, 0x5EED2003, 1.0, lambda: gs.rmat_stream(12, 60000, 24)),
+        (300, 0x5EED2004, 1.0, lambda: gs.er_stream(300, 0.05, 25, 0.1, 0.5)),
+    ]
+    assert gs.geometry_for(12).bkt_per_col < 10 <= gs.geometry_for(4096).bkt_per_col
+    with make_engine() as e:
+        ids, streams = [], []
+        for V, seed, f, gen in specs:
+            t = e.add_tenant(V, seed, f)
+            ids.append(t)
+            streams.append((t, gen()))
+        tens, offs, pairs = interleaved_slices(streams, 3, rng)
+        e.ingest(tens, offs, pairs)
+        res = e.connected_components(ids)
+        for (V, seed, f, _), (t, a) in zip(specs, streams):
+            sk, labels, ncc, rounds = solo(V, seed, f, a)
+            assert e.download(t).tobytes() == sk, t
+            assert np.array_equal(res[t].labels, labels), t
+            ref = restatement.new_sketches(V, f)
+            restatement.ingest(ref, V, seed, a, f)
+            assert e.download(t).tobytes() == ref.tobytes(), t
+
+
 def test_large_vertex_space_two_word_records(restatement):
     """In a 2^22-id vertex space a bucket-local key (11 bits) and a neighbour id (22 bits) do not fit one
     32-bit word, so the bucketing passes move (key, neighbour) pairs; the tenants' sketches and answers
