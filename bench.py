@@ -104,6 +104,13 @@ def ncu_issue_per_launch():
     return v, sha == kernel_source_sha16()
 
 
+def ncu_smem_per_launch():
+    """shared-memory wavefronts of one full-size ingest launch from the committed ncu summary, and
+    whether that capture ran the current kernel sources."""
+    v, sha = _profile_field("k_ingest_rmat17_issue.txt", "smem_wavefronts_per_full_launch")
+    return v, sha == kernel_source_sha16()
+
+
 def ncu_traffic_per_launch():
     """dram bytes read+write of one full-size ingest launch from the committed ncu summary, and whether
     that capture ran the current kernel sources."""
@@ -616,6 +623,19 @@ def run_gs(args):
                  "inst_per_launch": inst, "inst_source": "committed ncu capture (profiles/k_ingest_rmat17_issue.txt)",
                  "inst_capture_matches_source": inst_current, "kernel": "k_ingest_packed (sketch update)",
                  "peak_source": f"4 schedulers x {sms} SMs x median sampled SM clock"}
+    # ... and by shared-memory bandwidth: every (record, column) reads and writes a 16-byte row and every
+    # record is broadcast from the warp's stage; one wavefront (128 B) per SM and clock is the peak
+    smem = None
+    wf, wf_current = ncu_smem_per_launch()
+    if wf is not None and V == (1 << 17) and phase == (1 << 27) and clocks.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        ach = wf / (ingest_ms_avg / 1e3)
+        pk = 1.0 * sms * clocks["sm_mhz"] * 1e6
+        smem = {"bound": "shared-memory wavefronts", "achieved": ach, "peak": pk, "unit": "wavefronts/s",
+                "frac": ach / pk, "wavefronts_per_launch": wf,
+                "wavefront_source": "committed ncu capture (profiles/k_ingest_rmat17_issue.txt)",
+                "wavefront_capture_matches_source": wf_current, "kernel": "k_ingest_packed (sketch update)",
+                "peak_source": f"one 128-byte wavefront per SM and clock x {sms} SMs x median sampled SM clock"}
     split = {"ingest_ms_per_step": prof["ingest_ms"] / args.steps, "bucket_ms_per_step": prof["bucket_ms"] / args.steps,
              "query_ms_per_step": prof["query_ms"] / args.steps}
 
@@ -690,7 +710,7 @@ def run_gs(args):
                    "stream_seed": f"{STREAM_SEED:#x}+rank", "sketch_seed": f"{SKETCH_SEED:#x}+rank",
                    "sketch_bytes_per_vertex": Sv, "l2": "inputs larger than L2 (8 GiB of records per GPU)",
                    "parallelism": f"replicas x{world}", "tuning": tuning},
-        "roofline": roofline, "issue_roofline": issue, "cpu_baseline": cpu, "e2e": e2e,
+        "roofline": roofline, "issue_roofline": issue, "smem_roofline": smem, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": prof["kernel_launches"],
         "clocks": clocks, "kernel_split": split, "batched": batched, "served": served,
         "mincut": mincut, "dropin": dropin,

@@ -254,7 +254,7 @@ size_t part_scatter_staged_smem(uint32_t H) {
 // both whenever every neighbour id is below 2^(32 - lb) (V = 2^17: 9 + 17 bits); pass 2 then reads
 // 4 bytes per record instead of 8.
 template <bool COMPACT>
-__global__ void __launch_bounds__(kPartThreads) k_part_scatter_staged(const uint2* __restrict__ pairs, uint64_t n,
+__global__ void __launch_bounds__(kPartThreads, 3) k_part_scatter_staged(const uint2* __restrict__ pairs, uint64_t n,
                                                                       PairTag t, uint32_t lb, uint32_t H,
                                                                       uint32_t* __restrict__ bkt,
                                                                       uint2* __restrict__ part, uint64_t cap,
