@@ -73,13 +73,18 @@ KERNEL_SOURCES = ("gpusketch_b200/csrc/gs_ingest.cu", "gpusketch_b200/csrc/gs_co
 
 
 def kernel_source_sha16() -> str:
-    """sha256 (first 16 hex digits) of the sketch-update kernel's sources, as the ncu summaries record
-    it: a committed capture describes the current kernel only when the two agree."""
+    """sha256 (first 16 hex digits) of the sketch-update kernel's sources with comments and blank
+    lines removed, as the ncu summaries record it: a committed capture describes the current kernel
+    only when the two agree (an edit of a comment leaves the code, and the capture, current)."""
     import hashlib
+    import re
     h = hashlib.sha256()
     for rel in KERNEL_SOURCES:
-        with open(os.path.join(ROOT, rel), "rb") as f:
-            h.update(f.read())
+        with open(os.path.join(ROOT, rel), encoding="utf-8") as f:
+            text = f.read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        lines = (re.sub(r"//.*$", "", ln).rstrip() for ln in text.splitlines())
+        h.update("\n".join(ln for ln in lines if ln).encode())
     return h.hexdigest()[:16]
 
 

@@ -8,19 +8,19 @@
 //   2. k_part_scatter(_staged)       records placed by bucket: sorted per block in shared memory,
 //                                    then written as coalesced runs
 //   3. k_vert_count, k_scan_*        per-vertex record counts and work chunks ceil(count / chunk)
-//   4. k_vert_scatter                neighbours placed by vertex inside each chunk of a bucket
+//   4. k_vert_scatter(_sorted)       neighbours placed by vertex inside each chunk of a bucket
 //   5. k_ingest_packed / k_ingest    one warp per work chunk of one vertex.  A lane hashes the edge
 //                                    for one column (XXH3 with the column constant folded,
-//                                    gs_common.cuh) and XORs {mix(edge), checksum} into its own
-//                                    shared-memory row for that depth (depths < 10); deeper buckets
-//                                    (probability 2^-10) go straight to HBM with red.global.xor.
-//                                    k_ingest_packed (at most 32 columns) gives lanes left over by
-//                                    the columns the columns of a fourth record per three rounds;
-//                                    k_ingest (wider sketches, register depths) keeps lane = column.
-//                                    At the end of the chunk the non-zero rows and the deterministic
-//                                    bucket are merged into the vertex sketch (plain read-modify-
-//                                    write when the vertex is one chunk, atomic XOR when several
-//                                    warps share it).
+//                                    gs_common.cuh) and XORs {mix(edge), checksum} into the
+//                                    shared-memory row of that column and depth (depths < 10);
+//                                    deeper buckets (probability 2^-10) go straight to HBM with
+//                                    red.global.xor.  k_ingest_packed (at most 24 columns with the
+//                                    packed layout, up to 32 without) covers the columns of four
+//                                    records with 32 lanes in three steps; k_ingest (wider sketches,
+//                                    register depths) keeps lane = column.  At the end of the chunk
+//                                    the non-zero rows and the deterministic bucket are merged into
+//                                    the vertex sketch (plain read-modify-write when the vertex is
+//                                    one chunk, atomic XOR when several warps share it).
 //
 // XOR is commutative and associative, so the result is bit-identical to the reference's
 // sequential Sketch::update over the same records (src/sketch.cpp:85-99), whatever the order.
@@ -960,7 +960,7 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
   const uint32_t V = A.V;
   uint64_t csmix = 0, cmix = 0;
   // per lane: record slot of a group and, per step, column (>= C: none), column constant, row block
-  uint32_t ro = 0, sb[J], col[J], pitch = 0;
+  uint32_t ro = 0, sb[J], col[J], pitch = 0, msp = 0;
   uint64_t cm[J];
   auto set_geometry = [&](uint32_t c_new, const uint64_t* cmt) {
     C = c_new;
@@ -972,6 +972,8 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
     const uint32_t sl = se ? min(lane / se, J + 1) : J + 1, i = se ? lane % se : 0u;
     ro = min(sl, J);
     pitch = sl < J ? p1 : 8u;
+    // the merge's lane c < C: word of column c's spare rows (spare lane J se + c % se, step c / se)
+    msp = se && lane < C ? kRA * p1 + (lane / se) * kRA * 8u + ((J * se + lane % se) & 7u) : 0u;
 #pragma unroll
     for (uint32_t j = 0; j < J; j++) {
       const uint32_t c = sl < J ? i + se * ((j + sl) % J) : (sl == J ? i + se * j : 0xffffffffu);
@@ -1156,21 +1158,21 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
       __syncwarp();
     }
 
-    // merge: item i -> column i / kRows, depth i % kRows, so consecutive lanes cover contiguous
-    // buckets of one column; a column's spare slot (if any) is folded in first
-    for (uint32_t i = lane; i < C * kRows; i += 32) {
-      const uint32_t cl = i / kRows, row = i % kRows;
-      uint4 t = wbase[row * p1 + cl];
-      if (se) {
-        const uint32_t j = cl / se, sl = J * se + (cl - j * se);
-        const uint4 t2 = wbase[kRA * p1 + (j * kRA + row) * 8u + (sl & 7u)];
-        t.x ^= t2.x; t.y ^= t2.y; t.z ^= t2.z; t.w ^= t2.w;
+    // merge: one depth at a time, lane c on column c, so a quarter-warp reads eight columns of one
+    // row (eight bank groups); a column's spare rows (if any) are folded in first
+    if (lane < C) {
+      for (uint32_t row = 0; row < cap; row++) {
+        uint4 t = wbase[row * p1 + lane];
+        if (se) {
+          const uint4 t2 = wbase[msp + row * 8u];
+          t.x ^= t2.x; t.y ^= t2.y; t.z ^= t2.z; t.w ^= t2.w;
+        }
+        if ((t.x | t.y | t.z | t.w) == 0u) continue;
+        const uint64_t a = gs_key_unmix(((uint64_t)t.y << 32) | t.x), gm = ((uint64_t)t.w << 32) | t.z;
+        GsBucket* p = skv + (size_t)lane * bkt + row;
+        if (exclusive) { p->alpha ^= a; p->gamma ^= gm; }
+        else xor_bucket_global(p, a, gm);
       }
-      if (row >= bkt || (t.x | t.y | t.z | t.w) == 0u) continue;
-      const uint64_t a = gs_key_unmix(((uint64_t)t.y << 32) | t.x), gm = ((uint64_t)t.w << 32) | t.z;
-      GsBucket* p = skv + (size_t)cl * bkt + row;
-      if (exclusive) { p->alpha ^= a; p->gamma ^= gm; }
-      else xor_bucket_global(p, a, gm);
     }
     // deterministic bucket (last bucket of the sketch)
 #pragma unroll
