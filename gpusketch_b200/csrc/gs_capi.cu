@@ -23,7 +23,7 @@ void gs_free_graph(gs_graph* g) {
   if (!g) return;
   cudaFree(g->d_sk); cudaFree(g->d_colmix);
   cudaFree(g->d_cnt); cudaFree(g->d_off); cudaFree(g->d_choff); cudaFree(g->d_tile);
-  cudaFree(g->d_nbr); cudaFree(g->d_pairs); cudaFree(g->d_file_pairs); cudaFree(g->d_part); cudaFree(g->d_bkt); cudaFree(g->d_blockhist); cudaFree(g->d_chunkhist);
+  cudaFree(g->d_nbr); cudaFree(g->d_pairs); cudaFree(g->d_file_pairs); cudaFree(g->d_part); cudaFree(g->d_bkt); cudaFree(g->d_blockhist); cudaFree(g->d_chunkhist); cudaFree(g->d_owner);
   if (g->h_pin) cudaFreeHost(g->h_pin);
   if (g->h_status) cudaFreeHost(g->h_status);
   if (g->h_qstatus) cudaFreeHost(g->h_qstatus);

@@ -641,21 +641,41 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_top(uint32_t* __restrict_
   }
 }
 
-// adds the tile prefixes and resets the counters to the record cursors used by the scatter
+// adds the tile prefixes and resets the counters to the record cursors used by the scatter; with an
+// owner table, also records the vertex of each of its work chunks below owner_cap, so the sketch
+// update finds a chunk's vertex with one load instead of a search over choff
 __global__ void __launch_bounds__(kScanThreads) k_scan_add(uint32_t* __restrict__ off, uint32_t* __restrict__ choff,
                                                            uint32_t* __restrict__ cursor,
-                                                           const uint32_t* __restrict__ tile_sums, uint32_t nv) {
+                                                           const uint32_t* __restrict__ tile_sums, uint32_t nv,
+                                                           uint32_t chunk, uint32_t* __restrict__ owner,
+                                                           uint32_t owner_cap) {
   const uint32_t t = blockIdx.x;
   const uint32_t a = tile_sums[2 * t], b = tile_sums[2 * t + 1];
   const uint64_t base = (uint64_t)t * kScanTile + (uint64_t)threadIdx.x * kScanPer;
+  const uint32_t lane = threadIdx.x & 31u;
 #pragma unroll
   for (int k = 0; k < kScanPer; k++) {
-    uint64_t i = base + k;
+    const uint64_t i = base + k;
+    uint32_t c0 = 0, n = 0;
     if (i < nv) {
-      uint32_t o = off[i] + a;
+      const uint32_t o = off[i] + a;
       off[i] = o;
-      choff[i] += b;
+      c0 = choff[i] + b;
+      choff[i] = c0;
+      if (owner) n = (cursor[i] + chunk - 1) / chunk;   // cursor still holds the count here
       cursor[i] = o;
+    }
+    if (owner) {
+      // a vertex of a few chunks writes its own entries; the warp writes a hub vertex's together
+      constexpr uint32_t kOwnFew = 8;
+      if (n <= kOwnFew)
+        for (uint32_t c = c0; c < c0 + n && c < owner_cap; c++) owner[c] = (uint32_t)i;
+      for (uint32_t m = __ballot_sync(0xffffffffu, n > kOwnFew); m; m &= m - 1) {
+        const uint32_t src = __ffs(m) - 1;
+        const uint32_t hc0 = __shfl_sync(0xffffffffu, c0, src), hn = __shfl_sync(0xffffffffu, n, src);
+        const uint32_t hv = __shfl_sync(0xffffffffu, (uint32_t)i, src);
+        for (uint32_t c = hc0 + lane; c < hc0 + hn && c < owner_cap; c += 32) owner[c] = hv;
+      }
     }
   }
 }
@@ -674,6 +694,8 @@ struct IngestArgs {
   const GsIngTenant* tenants;    // geometry and arena offset of every tenant (tenant variant only)
   uint32_t warp_words;           // shared memory per warp in uint4 (packed variant only)
   uint32_t* next_chunk;          // work-chunk counter, zero at launch (packed variant only)
+  const uint32_t* owner;         // vertex of every work chunk below owner_cap (may be null)
+  uint32_t owner_cap;
 };
 
 // ---- packed lane layout (sketches of at most 24 columns) ----
@@ -805,8 +827,10 @@ __global__ void __launch_bounds__(512) k_ingest(const IngestArgs A) {
   for (uint32_t ch = dyn ? __shfl_sync(0xffffffffu, nxt, 0) : gw; ch < total;
        ch = dyn ? __shfl_sync(0xffffffffu, nxt, 0) : ch + nw) {
     if (dyn && lane == 0) nxt = atomicAdd(A.next_chunk, 1u);
-    const uint32_t vv = chunk_owner(A, ch, lane);
+    const uint32_t vv = ch < A.owner_cap ? A.owner[ch] : chunk_owner(A, ch, lane);
     const uint32_t c0 = A.choff[vv];
+    // a vertex of one chunk is this warp's alone: its merge is a plain read-modify-write (many small
+    // vertices, as an engine's tenants have, would saturate the L2 atomics)
     const bool exclusive = (A.choff[vv + 1] - c0) == 1;
     const uint32_t rb = A.off[vv] + (ch - c0) * A.chunk;
     const uint32_t re = min(A.off[vv + 1], rb + A.chunk);
@@ -993,9 +1017,8 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
   if (lane == 0) nxt = atomicAdd(A.next_chunk, 1u);
   for (uint32_t ch = __shfl_sync(0xffffffffu, nxt, 0); ch < total; ch = __shfl_sync(0xffffffffu, nxt, 0)) {
     if (lane == 0) nxt = atomicAdd(A.next_chunk, 1u);
-    const uint32_t vv = chunk_owner(A, ch, lane);
+    const uint32_t vv = ch < A.owner_cap ? A.owner[ch] : chunk_owner(A, ch, lane);
     const uint32_t c0ff = A.choff[vv];
-    const bool exclusive = (A.choff[vv + 1] - c0ff) == 1;
     const uint32_t rb = A.off[vv] + (ch - c0ff) * A.chunk;
     const uint32_t re = min(A.off[vv + 1], rb + A.chunk);
     uint32_t v, vb = 0;
@@ -1170,8 +1193,7 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
         if ((t.x | t.y | t.z | t.w) == 0u) continue;
         const uint64_t a = gs_key_unmix(((uint64_t)t.y << 32) | t.x), gm = ((uint64_t)t.w << 32) | t.z;
         GsBucket* p = skv + (size_t)lane * bkt + row;
-        if (exclusive) { p->alpha ^= a; p->gamma ^= gm; }
-        else xor_bucket_global(p, a, gm);
+        xor_bucket_global(p, a, gm);
       }
     }
     // deterministic bucket (last bucket of the sketch)
@@ -1183,8 +1205,7 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2) k_ingest_packed(const Inge
     if (lane == 0 && (det_m | det_g) != 0ull) {
       GsBucket* p = skv + (nb - 1);
       const uint64_t a = gs_key_unmix(det_m);
-      if (exclusive) { p->alpha ^= a; p->gamma ^= det_g; }
-      else xor_bucket_global(p, a, det_g);
+      xor_bucket_global(p, a, det_g);
     }
     __syncwarp();
   }
@@ -1202,6 +1223,8 @@ gs_status launch_ingest(gs_graph* g, uint32_t nv, cudaStream_t s) {
   A.bkt = g->geom.bkt_per_col; A.nb = g->geom.num_buckets; A.chunk = g->tune.chunk;
   A.warp_words = 0;
   A.next_chunk = g->d_status + 14;
+  A.owner = g->d_owner;
+  A.owner_cap = (uint32_t)g->owner_cap;
   const int warps = (int)g->tune.warps_per_block;
   const size_t smem = ingest_smem_bytes(CG, R, warps);
   // the opt-in shared-memory limit is a per-device function attribute; the persistent grid fills
@@ -1243,6 +1266,8 @@ gs_status launch_ingest_packed(gs_graph* g, uint32_t nv, cudaStream_t s) {
   A.tenants = TEN ? g->d_ten : nullptr;
   A.warp_words = packed_warp_words(g);
   A.next_chunk = g->d_status + 14;
+  A.owner = g->d_owner;
+  A.owner_cap = (uint32_t)g->owner_cap;
   const int warps = std::min(kPackMaxThreads / 32, (int)g->tune.warps_per_block);
   const size_t smem = (size_t)warps * A.warp_words * sizeof(uint4);
   struct Cache { size_t smem = 0; int warps = 0; int blocks = 0; };
@@ -1391,20 +1416,38 @@ static gs_status ensure_chunkhist(gs_graph* g, uint64_t records, uint32_t** out)
   return GS_OK;
 }
 
+// The chunk-owner table: a chunk per vertex with records plus one per `chunk` records, the records
+// bounded by the neighbour scratch.  A smaller table is never wrong (the sketch update finds the
+// chunks past its end by search), so it is not grown while a stream is being captured.
+static gs_status ensure_owner_table(gs_graph* g) {
+  const uint64_t nv = (uint64_t)g->num_levels * g->V;
+  const uint64_t want = std::min<uint64_t>(nv + g->nbr_cap / std::max(1u, g->tune.chunk) + 1, 0xffffffffull);
+  if (g->owner_cap >= want || g->capturing) return GS_OK;
+  cudaFree(g->d_owner);
+  g->d_owner = nullptr;
+  g->owner_cap = 0;
+  GS_CUDA_TRY(cudaMalloc(&g->d_owner, want * sizeof(uint32_t)));
+  g->owner_cap = want;
+  return GS_OK;
+}
+
 gs_status gs_reserve_ingest(gs_graph* g, uint64_t edges) {
   const uint64_t m = std::min<uint64_t>(edges, g->max_batch_edges);
   GS_TRY(gs_ensure_ingest_scratch(g, std::max<uint64_t>(2 * m, 1)));
   GS_TRY(ensure_partition_scratch(g, std::max<uint64_t>(2 * m, 1)));
   uint32_t* unused = nullptr;
   GS_TRY(ensure_blockhist(g, m, &unused));
-  return ensure_chunkhist(g, 2 * m, &unused);
+  GS_TRY(ensure_chunkhist(g, 2 * m, &unused));
+  return ensure_owner_table(g);
 }
 
 static gs_status scan_counts(gs_graph* g, uint32_t nv, cudaStream_t s) {
   const uint32_t tiles = (nv + kScanTile - 1) / kScanTile;
+  GS_TRY(ensure_owner_table(g));
   k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(g->d_cnt, nv, g->tune.chunk, g->d_off, g->d_choff, g->d_tile);
   k_scan_top<<<1, kScanThreads, 0, s>>>(g->d_tile, tiles, g->d_off, g->d_choff, nv, g->d_status);
-  k_scan_add<<<tiles, kScanThreads, 0, s>>>(g->d_off, g->d_choff, g->d_cnt, g->d_tile, nv);
+  k_scan_add<<<tiles, kScanThreads, 0, s>>>(g->d_off, g->d_choff, g->d_cnt, g->d_tile, nv, g->tune.chunk, g->d_owner,
+                                            (uint32_t)g->owner_cap);
   GS_CUDA_TRY(cudaGetLastError());
   return GS_OK;
 }
@@ -1574,6 +1617,8 @@ gs_status launch_ingest_scratch(const GsScratchIngest& x, cudaStream_t s) {
   A.tenants = nullptr;
   A.warp_words = 0;
   A.next_chunk = nullptr;
+  A.owner = nullptr;
+  A.owner_cap = 0;
   const size_t smem = ingest_smem_bytes(CG, 1, (int)x.warps);
   int nb = 0;
   GS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ingest<CG, 1, SMALL, false>, (int)x.warps * 32, smem));
@@ -1606,7 +1651,7 @@ gs_status gs_ingest_pairs_on_scratch(const GsScratchIngest& x, cudaStream_t s) {
   const uint32_t stiles = (nv + kScanTile - 1) / kScanTile;
   k_scan_tiles<<<stiles, kScanThreads, 0, s>>>(x.cnt, nv, x.chunk, x.off, x.choff, x.tile);
   k_scan_top<<<1, kScanThreads, 0, s>>>(x.tile, stiles, x.off, x.choff, nv, x.status);
-  k_scan_add<<<stiles, kScanThreads, 0, s>>>(x.off, x.choff, x.cnt, x.tile, nv);
+  k_scan_add<<<stiles, kScanThreads, 0, s>>>(x.off, x.choff, x.cnt, x.tile, nv, x.chunk, nullptr, 0u);
   k_vert_scatter<false><<<grid2, kPartThreads, 2 * (1u << lb) * sizeof(uint32_t), s>>>(x.part, x.bkt, H, lb, x.cnt, x.nbr,
                                                                                 x.records_cap, x.status);
   GS_CUDA_TRY(cudaGetLastError());

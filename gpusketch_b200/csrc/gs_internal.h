@@ -85,6 +85,8 @@ struct gs_graph {
   uint64_t blockhist_cap = 0;
   uint32_t* d_chunkhist = nullptr;  // [chunks][2^lb] vertex counts of every pass-2 chunk
   uint64_t chunkhist_cap = 0;
+  uint32_t* d_owner = nullptr;      // [work chunk] vertex owning it, for the chunks below owner_cap
+  uint64_t owner_cap = 0;
   uint32_t part_buckets = 0;   // H
   uint32_t part_lb = 9;        // low key bits resolved by the second pass
   uint32_t* d_pairs = nullptr; // staging for host-resident input pairs, 2 x [pairs_cap] u32 pairs
