@@ -229,6 +229,45 @@ def test_vertex_batches_apply_to_source_only(restatement):
     assert got == sk.tobytes()
 
 
+@pytest.mark.parametrize("reg_depth", [0, 1])
+def test_device_vertex_batches_past_the_owner_table(restatement, reg_depth):
+    """Device-resident vertex batches are counted before the neighbour scratch grows to their size, so
+    the chunk-owner table (sized by that scratch) covers only the first work chunks; the sketch update
+    finds the vertex of every later chunk by search.  Small scratch, 32-record chunks: most chunks lie
+    past the table.  The bytes equal the restatement's, for the packed and the one-column kernel."""
+    import ctypes as C
+    import torch
+    from gpusketch_b200._native import check
+    from gpusketch_b200.autotune import set_tuning
+    V, seed = 512, 0x5EED0077
+    rng = np.random.default_rng(77)
+    srcs = rng.integers(0, V, 400).astype(np.uint32)
+    sizes = rng.integers(0, 500, 400).astype(np.uint64)
+    starts = np.zeros_like(sizes)
+    np.cumsum(sizes[:-1], out=starts[1:])
+    dsts = rng.integers(0, V, int(sizes.sum())).astype(np.uint32)
+    with gs.GraphSketch(V, seed, max_batch_edges=1024) as g:
+        set_tuning(g, 32, 8, reg_depth)
+        d_srcs = torch.from_numpy(srcs.astype(np.int32)).cuda()
+        d_starts = torch.from_numpy(starts.astype(np.int64)).cuda()
+        d_sizes = torch.from_numpy(sizes.astype(np.int64)).cuda()
+        d_dsts = torch.from_numpy(dsts.astype(np.int32)).cuda()
+        torch.cuda.synchronize()
+        check(g._lib.gs_ingest_vertex_batches(g._h, 0, d_srcs.data_ptr(), d_starts.data_ptr(), d_sizes.data_ptr(),
+                                              len(srcs), d_dsts.data_ptr(), len(dsts), 1, None),
+              "gs_ingest_vertex_batches")
+        g.synchronize()
+        got = sketch_bytes(g)
+    nb = restatement.geometry(V)["num_buckets"]
+    sk = restatement.new_sketches(V)
+    for b in range(len(srcs)):
+        s = int(srcs[b])
+        one = sk[s * nb * 2:(s + 1) * nb * 2]
+        for d in dsts[int(starts[b]):int(starts[b] + sizes[b])].tolist():
+            restatement.sketch_update(one, V, seed, (min(s, d) << 32) | max(s, d))
+    assert got == sk.tobytes()
+
+
 def test_linearity_and_self_inverse(restatement):
     V, seed = 3000, 2024
     rng = np.random.default_rng(7)
