@@ -690,17 +690,19 @@ def run_gs(args):
     g.close()
     del d_in
     torch.cuda.empty_cache()
+    # the one-GPU sub-lines (min cut, drop-in, batched, served) run at N=1 only: at N>1 they would
+    # hold every GPU for a minute of measurements the scaling line does not use
     batched = served = mincut = dropin = None
-    if not args.no_mincut:
+    if not args.no_mincut and world == 1:
         mincut = run_mincut(args, dev)
-    if not args.no_dropin and rank == 0:
+    if not args.no_dropin and world == 1:
         try:
             dropin = run_dropin(args, dev)
         except Exception as exc:  # a sub-line, never required
             dropin = {"error": str(exc)}
-    if not args.no_batched:
+    if not args.no_batched and world == 1:
         batched = run_batched(args, dev, max(1, args.steps), max(1, args.warmup))
-    if not args.no_served:
+    if not args.no_served and world == 1:
         served = run_served(args, dev)
     if dist is not None:
         dist.destroy_process_group()
