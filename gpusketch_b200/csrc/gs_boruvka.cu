@@ -173,7 +173,9 @@ __device__ bool grid_sync(uint32_t* count, uint32_t* gen, uint32_t* err, uint64_
       while (ld_volatile(gen) == g) {
         __nanosleep(sleep_ns);
         waited += sleep_ns;
-        if (sleep_ns < 1024) sleep_ns <<= 1;
+        // back-off capped at 256 ns: a block that waited long notices the release within a
+        // quarter microsecond (1024 ns made the 10-round query 1% slower)
+        if (sleep_ns < 256) sleep_ns <<= 1;
         if ((++it & 63u) == 0 && (ld_volatile(err) & GS_DEV_ERR_TIMEOUT)) { ok = 0; break; }
         if (waited > wait_ns) {
           atomicOr(err, (uint32_t)GS_DEV_ERR_TIMEOUT);
