@@ -569,10 +569,16 @@ def run_gs(args):
     g.clear()
 
     def step(src):
+        # each phase's query is queued behind its records and the next phase's records behind the
+        # query before its answer (labels, component count) is collected, so the device never idles
+        # while the host collects an answer; every phase is still ingested, queried and answered
         g.clear()
+        g.ingest_pairs(src[0:phase])
         for p in range(P):
-            g.ingest_pairs(src[p * phase:(p + 1) * phase])
-            g.connected_components()
+            g.connected_components_async()
+            if p + 1 < P:
+                g.ingest_pairs(src[(p + 1) * phase:(p + 2) * phase])
+            g.query_wait()
 
     def barrier():
         rank_barrier(dist)
