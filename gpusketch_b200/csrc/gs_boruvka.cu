@@ -583,7 +583,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_boruvka(const BorArgs A) {
       if (e == ~0ull) continue;
       const uint32_t gs = (uint32_t)(e >> 32), gd = (uint32_t)e;
       if (dsu_union(A.parent, gs, gd, limit, err)) {
-        A.tstate[4 * t + 1] = 1u;
+        // read before writing: with one graph every successful union (2^17 in round 0 at V=2^17)
+        // would store to the same flag, and those stores queue on one L2 line
+        if (!ld_volatile(&A.tstate[4 * t + 1])) A.tstate[4 * t + 1] = 1u;
         const uint32_t f = atomicAdd(&A.status[4], 1u);
         if (f < A.forest_cap) {
           A.forest[2 * f] = min(gs, gd);
